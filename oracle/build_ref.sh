@@ -1,0 +1,31 @@
+#!/usr/bin/env bash
+# Builds the reference DREAM delay-and-sum CPU implementation, unmodified, from
+# its own sources into oracle/_ref/ as the pybind11 modules `das` (FP64) and
+# `das_f` (FP32). These modules are test infrastructure: they pin the oracle
+# and serve as the timed CPU baseline. Nothing on the product path loads them.
+#
+# Sources compiled (paths inside the reference tree):
+#   python/src/py_das.cc  extra_src/das.cc  src/affinity.cc  src/dream_error.cc
+# Flags: -O3 -ffp-contract=off, no -march=native, so the x86-64 baseline ISA
+# (no FMA) computes every product and sum exactly as written.
+#
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+set -euo pipefail
+REF="${1:-/root/reference}"
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+OUT="$HERE/_ref"
+if [ ! -f "$REF/extra_src/das.cc" ]; then
+  echo "build_ref: reference sources not found under $REF" >&2
+  exit 1
+fi
+PY="${PYTHON:-python3}"
+PYINC="$($PY -c 'import sysconfig; print(sysconfig.get_paths()["include"])')"
+PBINC="$($PY -c 'import pybind11; print(pybind11.get_include())')"
+EXT="$($PY -c 'import sysconfig; print(sysconfig.get_config_var("EXT_SUFFIX"))')"
+mkdir -p "$OUT"
+SRCS=("$REF/python/src/py_das.cc" "$REF/extra_src/das.cc" "$REF/src/affinity.cc" "$REF/src/dream_error.cc")
+FLAGS=(-O3 -ffp-contract=off -std=c++14 -shared -fPIC -DDREAM_PYTHON
+       -I "$REF/include" -I "$REF/python/include" -I "$PYINC" -I "$PBINC" -lpthread)
+g++ "${FLAGS[@]}" "${SRCS[@]}" -o "$OUT/das$EXT"
+g++ "${FLAGS[@]}" -DUSE_FLOAT "${SRCS[@]}" -o "$OUT/das_f$EXT"
+echo "build_ref: built $OUT/das$EXT and $OUT/das_f$EXT"

@@ -1,0 +1,174 @@
+"""ctypes front end of the C restatement of the reference DAS (das_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py as the checker. The product path never imports it.
+
+Also exposes the unmodified reference modules built by oracle/build_ref.sh
+(``reference_module``) when they are present.
+"""
+from __future__ import annotations
+
+import ctypes
+import glob
+import importlib.util
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdas_oracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+
+METHODS = {"saft": 0, "tfm": 1, "rca": 2, "rca_coltx": 2, "rca_rowtx": 3}
+ERR_LEVELS = {"none": 0, "ignore": 1, "warn": 2, "stop": 3}
+OOB_MISS = np.iinfo(np.int64).min
+
+_lib = None
+
+
+def build() -> str:
+    """Compiles das_oracle.c with gcc (make) if the shared object is stale."""
+    src = os.path.join(HERE, "das_oracle.c")
+    if (not os.path.exists(LIB_PATH)) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(LIB_PATH)
+        i64, i32, vp = ctypes.c_int64, ctypes.c_int, ctypes.c_void_p
+        f64, f32 = ctypes.c_double, ctypes.c_float
+        L.dream_oracle_das_f64.argtypes = [i32, vp, i64, vp, i64, vp, i64, vp, i64, f64, i32, vp,
+                                           f64, i32, vp, vp, vp]
+        L.dream_oracle_das_f32.argtypes = [i32, vp, i64, vp, i64, vp, i64, vp, i64, f32, i32, vp,
+                                           f32, i32, vp, vp, vp]
+        L.dream_oracle_das_uni_f64.argtypes = [i32, vp, i64, vp, f64, f64, f64, i32, vp, vp]
+        L.dream_oracle_das_uni_f32.argtypes = [i32, vp, i64, vp, f32, f32, f32, i32, vp, vp]
+        L.dream_oracle_uni_count_f64.argtypes = [f64, f64, f64]
+        L.dream_oracle_uni_count_f64.restype = i64
+        L.dream_oracle_uni_count_f32.argtypes = [f32, f32, f32]
+        L.dream_oracle_uni_count_f32.restype = i64
+        for n in ("dream_oracle_das_weighted_f64", "dream_oracle_das_adjoint_f64"):
+            getattr(L, n).argtypes = [vp, i64, i64, i64, vp, vp, vp]
+        L.dream_oracle_das_wgrad_f64.argtypes = [vp, i64, i64, i64, vp, vp, vp]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def das(Y, Gt, Gr, Ro, dt, delay, cp, method="tfm", err_level="ignore", dtype=np.float64,
+        return_idx=False):
+    """Oracle ``das``: returns ``(Im, status, oob_count[, idx])``.
+
+    ``dtype`` float64 restates ``das`` (DAS<double>), float32 restates
+    ``das_f`` (DAS<float>). ``idx`` is ``(terms, No)`` int64 with
+    ``OOB_MISS`` for out-of-bounds terms.
+    """
+    dt_ = np.dtype(dtype)
+    c = lambda a: np.asfortranarray(np.asarray(a, dtype=dt_))
+    Y, Gt, Ro = c(Y), c(Gt), c(Ro)
+    Gr = c(Gr) if Gr is not None and np.size(Gr) else np.zeros((0, 3), dtype=dt_, order="F")
+    delay = c(np.atleast_1d(np.asarray(delay)).reshape(-1))
+    K, No, Nt = Y.shape[0], Ro.shape[0], Gt.shape[0]
+    m = METHODS[method]
+    Nr = 0 if m == 0 else Gr.shape[0]
+    if Nr == 0:
+        m = 0
+    multi = 1 if delay.size != 1 else 0
+    Im = np.zeros(No, dtype=dt_)
+    oob = ctypes.c_int64(0)
+    idx = None
+    if return_idx:
+        terms = Nt if m == 0 else Nt * Nr
+        idx = np.zeros((terms, No), dtype=np.int64)
+    fn = lib().dream_oracle_das_f64 if dt_ == np.float64 else lib().dream_oracle_das_f32
+    st = fn(m, _p(Y), K, _p(Ro), No, _p(Gt), Nt, _p(Gr), Nr, dt, multi, _p(delay), cp,
+            ERR_LEVELS[err_level], _p(Im), ctypes.byref(oob), _p(idx))
+    if return_idx:
+        return Im, st, oob.value, idx
+    return Im, st, oob.value
+
+
+def uni_count(mn, d, mx, dtype=np.float64) -> int:
+    if np.dtype(dtype) == np.float64:
+        return int(lib().dream_oracle_uni_count_f64(mn, d, mx))
+    return int(lib().dream_oracle_uni_count_f32(mn, d, mx))
+
+
+def das_uni(Y, gt, gr, ro, dt, delay, cp, method="tfm", err_level="ignore", dtype=np.float64):
+    """Oracle ``das_uni`` (the reference's OpenCL kernels restated on the CPU).
+
+    ``gt``/``gr`` are ``[min, pitch, max]``; ``ro`` is 3x3 with rows x, y, z and
+    columns (min, d, max). Returns ``(Im, status, oob_count)``.
+    """
+    dt_ = np.dtype(dtype)
+    Y = np.asfortranarray(np.asarray(Y, dtype=dt_))
+    gt = np.asarray(gt, dtype=dt_).reshape(-1)
+    gr = np.asarray(gr, dtype=dt_).reshape(-1) if gr is not None and np.size(gr) else np.zeros(3, dt_)
+    ro = np.asarray(ro, dtype=dt_).reshape(3, 3)
+    tri = np.concatenate([gt, gr, ro[0], ro[1], ro[2]]).astype(dt_)
+    m = METHODS[method]
+    if m != 0 and np.size(gr) == 0:
+        m = 0
+    cnt = lambda a, b, c: uni_count(a, b, c, dt_)
+    No = cnt(*ro[0]) * cnt(*ro[1]) * cnt(*ro[2])
+    Im = np.zeros(No, dtype=dt_)
+    oob = ctypes.c_int64(0)
+    fn = lib().dream_oracle_das_uni_f64 if dt_ == np.float64 else lib().dream_oracle_das_uni_f32
+    d0 = float(np.asarray(delay).reshape(-1)[0])
+    st = fn(m, _p(Y), Y.shape[0], _p(tri), dt, d0, cp, ERR_LEVELS[err_level], _p(Im),
+            ctypes.byref(oob))
+    return Im, st, oob.value
+
+
+def weighted(idx, Y, w):
+    """``Im[o] = sum_c w[c] * Y[idx[c, o], c]`` on an oracle index table."""
+    idx = np.ascontiguousarray(idx, dtype=np.int64)
+    Y = np.asfortranarray(Y, dtype=np.float64)
+    w = np.ascontiguousarray(w, dtype=np.float64).reshape(-1)
+    C, No = idx.shape
+    Im = np.zeros(No)
+    lib().dream_oracle_das_weighted_f64(_p(idx), No, C, Y.shape[0], _p(Y), _p(w), _p(Im))
+    return Im
+
+
+def adjoint(idx, x, w, K):
+    """``Ya[idx[c, o], c] += w[c] * x[o]``: the adjoint of :func:`weighted`."""
+    idx = np.ascontiguousarray(idx, dtype=np.int64)
+    x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+    w = np.ascontiguousarray(w, dtype=np.float64).reshape(-1)
+    C, No = idx.shape
+    Ya = np.zeros((K, C), order="F")
+    lib().dream_oracle_das_adjoint_f64(_p(idx), No, C, K, _p(x), _p(w), _p(Ya))
+    return Ya
+
+
+def wgrad(idx, g, Y):
+    """``dw[c] = sum_o g[o] * Y[idx[c, o], c]``."""
+    idx = np.ascontiguousarray(idx, dtype=np.int64)
+    g = np.ascontiguousarray(g, dtype=np.float64).reshape(-1)
+    Y = np.asfortranarray(Y, dtype=np.float64)
+    C, No = idx.shape
+    dw = np.zeros(C)
+    lib().dream_oracle_das_wgrad_f64(_p(idx), No, C, Y.shape[0], _p(g), _p(Y), _p(dw))
+    return dw
+
+
+def reference_module(precision: str = "f64"):
+    """The unmodified reference module (``das`` or ``das_f``) from oracle/_ref, or None."""
+    name = "das" if precision == "f64" else "das_f"
+    hits = glob.glob(os.path.join(REF_DIR, name + ".cpython-*.so"))
+    if not hits:
+        return None
+    spec = importlib.util.spec_from_file_location(name, hits[0])
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
