@@ -1,0 +1,362 @@
+#!/usr/bin/env python
+"""DAS beamformer benchmark on B200: pixel x tx x rx sums per second.
+
+Workload (one "step"): one delay-and-sum frame of the TFM full-matrix-capture
+configuration -- 64 x 64 elements (pitch 0.5 mm), K = 3000 samples
+(dt = 0.04 us, cp = 1500 m/s), 512 x 512 image (x in [-20, 20] mm,
+z in [2, 50] mm) = 1.074e9 sums -- on seeded synthetic A-scans.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Each rank beamforms its own frame (frames are independent: weak scaling, no
+data-path collective). One JSON line is printed by rank 0.
+
+value : whole-job Gsum/s with inputs resident in HBM (CUDA events on the
+        launching stream, L2 flushed between steps by writing 256 MiB).
+e2e   : the same metric through the public API (dream_b200.das_f.das) from
+        pinned host arrays: H2D of the inputs and D2H of the image each step.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DAS Gsum/s (pixel x tx x rx)"
+WORKLOAD = "TFM FMC 64x64 elements, K=3000, 512x512 image"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def make_scene(rank: int):
+    from dream_b200 import synth
+    return synth.tfm_scene(seed=1 + rank)
+
+
+def cpu_baseline(scene, budget_s: float = 20.0):
+    """The reference das_f (built from the reference sources into oracle/_ref)
+    on the host cores; falls back to the C restatement (single thread) on a
+    pixel sample when the reference build is absent."""
+    from oracle import oracle
+    nproc = os.cpu_count() or 1
+    os.environ["DREAM_NUM_THREADS"] = str(nproc)
+    s = scene.astype(np.float32)
+    mod = oracle.reference_module("f32")
+    if mod is not None:
+        best, runs, t_all = None, 0, time.perf_counter()
+        while runs < 3 and (time.perf_counter() - t_all) < budget_s:
+            t0 = time.perf_counter()
+            mod.das(s.Y, s.Gt, s.Gr, s.Ro, np.float32(s.dt), s.delay, np.float32(s.cp), "tfm", "ignore", "cpu", "")
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+            runs += 1
+        return {"value": s.sums / best / 1e9, "unit": "Gsum/s", "cores": nproc, "kind": "reference",
+                "sample": f"full frame ({s.sums} sums), best of {runs}, reference das_f with "
+                          f"DREAM_NUM_THREADS={nproc}"}
+    n = 2048
+    sel = np.random.default_rng(0).choice(s.Ro.shape[0], n, replace=False)
+    t0 = time.perf_counter()
+    oracle.das(s.Y, s.Gt, s.Gr, np.asfortranarray(s.Ro[sel]), np.float32(s.dt), s.delay, np.float32(s.cp),
+               "tfm", "ignore", np.float32)
+    dt = time.perf_counter() - t0
+    sums = n * s.Gt.shape[0] * s.Gr.shape[0]
+    return {"value": sums / dt / 1e9, "unit": "Gsum/s", "cores": 1, "kind": "port",
+            "sample": f"{n} random pixels of the frame ({sums} sums), C restatement, 1 thread"}
+
+
+def run_reference(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return
+    from oracle import oracle
+    nproc = os.cpu_count() or 1
+    os.environ["DREAM_NUM_THREADS"] = str(nproc)
+    s = make_scene(0).astype(np.float32)
+    mod = oracle.reference_module("f32")
+    kind = "reference" if mod is not None else "port"
+    Ro = s.Ro
+    sums = s.sums
+
+    def step():
+        if mod is not None:
+            mod.das(s.Y, s.Gt, s.Gr, Ro, np.float32(s.dt), s.delay, np.float32(s.cp), "tfm", "ignore", "cpu", "")
+        else:
+            oracle.das(s.Y, s.Gt, s.Gr, Ro, np.float32(s.dt), s.delay, np.float32(s.cp), "tfm", "ignore",
+                       np.float32)
+
+    t0 = time.perf_counter()
+    step()
+    first = time.perf_counter() - t0
+    sample = "full frame"
+    if first * (args.steps + args.warmup) > 150.0 or mod is None:
+        # bound the run: a seeded pixel subset of the frame
+        n = max(256, int(Ro.shape[0] * min(1.0, 150.0 / max(first, 1e-3) / (args.steps + args.warmup))))
+        if mod is None:
+            n = min(n, 2048)
+        sel = np.sort(np.random.default_rng(0).choice(s.Ro.shape[0], n, replace=False))
+        Ro = np.asfortranarray(s.Ro[sel])
+        sums = n * s.Gt.shape[0] * s.Gr.shape[0]
+        sample = f"{n} seeded pixels of the frame"
+    for _ in range(max(0, args.warmup - 1)):
+        step()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    val = sums * args.steps / tot / 1e9
+    cores = nproc if mod is not None else 1
+    line = {"metric": METRIC, "value": val, "unit": "Gsum/s", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scatterers + noise)",
+            "config": {"workload": WORKLOAD, "global_batch": 1, "precision": "das_f (FP32)"},
+            "cpu_baseline": {"value": val, "unit": "Gsum/s", "cores": cores, "kind": kind,
+                             "sample": f"{sample}, {sums} sums per step, DREAM_NUM_THREADS={nproc}"},
+            "e2e": {"value": val, "unit": "Gsum/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def read_traffic(kernel_key: str):
+    """Per-launch DRAM bytes of a kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel_key and not line.startswith("#"):
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    from dream_b200 import _lib, das_f
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    L = _lib.load()
+
+    scene = make_scene(rank)
+    s32 = scene.astype(np.float32)
+    K, C = s32.Y.shape
+    No, Nt, Nr = s32.Ro.shape[0], s32.Gt.shape[0], s32.Gr.shape[0]
+    sums = s32.sums
+
+    def dev_f(a, dt):  # column-major device copy
+        return torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=dt).T)).to(dev).t()
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    d_oob = torch.zeros(1, dtype=torch.int64, device=dev)
+
+    def variant(prec_code, np_dt, steps, warmup):
+        Y, Gt, Gr, Ro = (dev_f(a, np_dt) for a in (s32.Y if np_dt == np.float32 else scene.Y, scene.Gt,
+                                                     scene.Gr, scene.Ro))
+        delay = dev_f(np.zeros((1, 1)), np_dt)
+        Im = torch.empty(No, dtype=Y.dtype, device=dev)
+        plan = _lib.plan_create(_lib.TFM, K, No, Nt, Nr, prec_code, local)
+        ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+        args_ = (plan.handle, ptr(Y), ptr(Ro), ptr(Gt), ptr(Gr), float(np_dt(scene.dt)), _lib.DELAY_SINGLE,
+                 ptr(delay), float(np_dt(scene.cp)), ptr(Im), ctypes.c_void_p(d_oob.data_ptr()),
+                 ctypes.c_void_p(stream.cuda_stream))
+
+        def launch():
+            _lib.check(L.dream_das_run_device_async(*args_))
+
+        for _ in range(warmup):
+            flush.fill_(1.0)
+            launch()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        n0 = L.dream_das_plan_launch_count(plan.handle)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for i in range(steps):
+            flush.fill_(float(i))  # 256 MiB write: evicts Y (49 MB FP32) from the 126 MB L2
+            evs[i][0].record(stream)
+            launch()
+            evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        launches = L.dream_das_plan_launch_count(plan.handle) - n0
+        ms = [a.elapsed_time(b) for a, b in evs]
+        tot = torch.tensor([sum(ms)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+        if int(d_oob.item()) != 0:
+            raise RuntimeError("unexpected out-of-bounds terms in the benchmark scene")
+        return float(tot.item()), ms, launches, Im
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    tot32, ms32, launches32, Im32 = variant(_lib.PREC_F32, np.float32, args.steps, args.warmup)
+    clk = clocks.stop()
+    f64_steps = max(3, args.steps // 4)
+    tot64, ms64, launches64, _ = variant(_lib.PREC_F64, np.float64, f64_steps, max(3, args.warmup // 2))
+
+    step_ms = tot32 / args.steps
+    value = world * sums / (step_ms * 1e-3) / 1e9
+    value64 = world * sums / (tot64 / f64_steps * 1e-3) / 1e9
+
+    # ---- e2e through the public API from pinned host memory ----
+    def pinned_f(a, dt):
+        a = np.asarray(a, dtype=dt)
+        t = torch.empty(a.shape[::-1], dtype=torch.float32 if dt == np.float32 else torch.float64,
+                        pin_memory=True)
+        arr = t.numpy().T
+        arr[...] = a
+        return arr
+
+    hY, hGt, hGr, hRo = (pinned_f(a, np.float32) for a in (s32.Y, s32.Gt, s32.Gr, s32.Ro))
+    hdelay = pinned_f(np.zeros((1, 1)), np.float32)
+    e2e_steps = max(3, args.steps // 2)
+    for _ in range(2):
+        das_f.das(hY, hGt, hGr, hRo, np.float32(s32.dt), hdelay, np.float32(s32.cp), "tfm", "ignore", "cuda")
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        out = das_f.das(hY, hGt, hGr, hRo, np.float32(s32.dt), hdelay, np.float32(s32.cp), "tfm", "ignore",
+                        "cuda")
+    t_e2e = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
+    e2e_val = world * sums * e2e_steps / float(t_e2e.item()) / 1e9
+    h2d = hY.nbytes + hGt.nbytes + hGr.nbytes + hRo.nbytes + hdelay.nbytes
+    d2h = out.nbytes + 8
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    peak, peak_kind = measured_peaks()
+    gathered = sums * 4  # one FP32 sample gathered per sum
+    achieved = gathered / (step_ms * 1e-3) / 1e9
+    compulsory = s32.Y.nbytes + s32.Ro.nbytes + No * 4 + (Nt + Nr) * 12
+    line = {
+        "metric": METRIC, "value": value, "unit": "Gsum/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded point scatterers, Gaussian-windowed 5 MHz sine, N(0,0.01) noise)",
+        "config": {"workload": WORKLOAD, "global_batch": world, "frames_per_gpu": 1,
+                   "precision": "plain FP32 (bit-exact with reference das_f)",
+                   "l2": "flushed between timed steps (256 MiB write, outside the timed events)",
+                   "parallelism": f"{world} independent frames, one per GPU"},
+        "variants": {
+            "plain_f32": {"gsum_s": value, "ms_per_frame": step_ms},
+            "plain_f64": {"gsum_s": value64, "ms_per_frame": tot64 / f64_steps},
+        },
+        "e2e": {"value": e2e_val, "unit": "Gsum/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "api": "dream_b200.das_f.das(numpy arrays in pinned host memory, device='cuda')"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": read_traffic("das_plain_f32_tfm"),
+                     "peak_source": f"{peak_kind} hbm_gbs",
+                     "algorithmic_bytes_per_launch": gathered,
+                     "note": "achieved = gathered sample bytes (4 B per sum) / kernel time",
+                     "compulsory_hbm_frac": compulsory / (step_ms * 1e-3) / 1e9 / peak},
+        "gpu_launches": int(launches32),
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(scene)
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,527 @@
+// das_capi.cu -- the C ABI declared in include/dream_das.h.
+//
+// A plan plays the role of the reference's cached DAS<T> / DAS_UNI<T> object
+// (include/das.h:52-94, include/das_uni.h:50-64): it remembers the setup,
+// owns the device buffers the host-pointer entry points stage through, an
+// out-of-bounds counter and a stream. Argument checks follow the reference
+// bindings (python/include/py_das.hpp:53-148, include/arg_parser.h:236-290).
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "../../include/dream_das.h"
+#include "das_kernels.h"
+
+using namespace dream;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char *where) {
+  g_last_error = std::string(where) + ": " + cudaGetErrorString(e);
+  return DREAM_ERR_CUDA;
+}
+
+#define CU(call)                                       \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = true;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) ok = cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= cap) return 0;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    if (bytes == 0) return 0;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(DREAM_ERR_ALLOC, std::string("device allocation of ") + std::to_string(bytes) +
+                                       " bytes failed: " + cudaGetErrorString(e));
+    }
+    cap = bytes;
+    return 0;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+int status_from_oob(uint64_t oob, int err_level) {
+  if (oob == 0) return DREAM_STATUS_NONE;
+  switch (err_level) {  // src/dream_error.cc:40-76
+    case DREAM_ERR_LEVEL_IGNORE: return DREAM_STATUS_IGNORE_OUT_OF_BOUNDS;
+    case DREAM_ERR_LEVEL_WARN: return DREAM_STATUS_WARN_OUT_OF_BOUNDS;
+    case DREAM_ERR_LEVEL_STOP:
+    case DREAM_ERR_LEVEL_PARALLEL_STOP: return DREAM_STATUS_OUT_OF_BOUNDS;
+    default: return DREAM_STATUS_NONE;
+  }
+}
+
+}  // namespace
+
+struct dream_das_plan {
+  int das_type = 0;
+  int64_t K = 0, No = 0, Nt = 0, Nr = 0;
+  int precision = 0;
+  int device = 0;
+  bool uni = false;
+  double tri[15] = {0};
+  int64_t Nx = 0, Ny = 0, Nz = 0;
+  cudaStream_t stream = nullptr;
+  DevBuf bY, bRo, bGt, bGr, bDelay, bIm, bOob;
+  unsigned long long *h_oob = nullptr;  // pinned
+  std::atomic<bool> cancelled{false};
+  std::atomic<int64_t> launches{0};
+  std::mutex mu;
+};
+
+namespace {
+
+size_t prec_size(int prec) { return prec == DREAM_PREC_F64 ? 8 : 4; }
+
+int check_common(int das_type, int64_t K, int64_t No, int64_t Nt, int64_t Nr, int precision) {
+  if (das_type < DREAM_DAS_SAFT || das_type > DREAM_DAS_RCA_ROWTX)
+    return fail(DREAM_ERR_ARGUMENT, "Unknown delay-and-sum method!");
+  if (K < 0 || No < 0 || Nt < 0 || Nr < 0) return fail(DREAM_ERR_ARGUMENT, "negative size");
+  if (precision < DREAM_PREC_F64 || precision > DREAM_PREC_BF16_STORE)
+    return fail(DREAM_ERR_ARGUMENT, "unknown precision");
+  if (K > INT32_MAX) return fail(DREAM_ERR_ARGUMENT, "A-scan length must be below 2^31 samples");
+  if (precision == DREAM_PREC_F32 && K > (int64_t(1) << 24))
+    return fail(DREAM_ERR_ARGUMENT, "FP32 plans need A-scans of at most 2^24 samples");
+  if (Nt > INT32_MAX || Nr > INT32_MAX) return fail(DREAM_ERR_ARGUMENT, "too many elements");
+  return 0;
+}
+
+// RCA stripe edges are read as Gr[Nt], Gr[2*Nt-1], Gt[0], Gt[Nr-1]
+// (extra_src/das.cc:464-467); these must lie inside the 3*Nr and 3*Nt arrays.
+int check_rca_edges(int64_t Nt, int64_t Nr) {
+  if (Nt < 1 || Nr < 1) return fail(DREAM_ERR_ARGUMENT, "RCA needs at least one column and one row");
+  if (2 * Nt - 1 >= 3 * Nr || Nr - 1 >= 3 * Nt)
+    return fail(DREAM_ERR_ARGUMENT,
+                "RCA stripe edges would be read outside Gt/Gr (the reference reads "
+                "Gr[num_cols], Gr[2*num_cols-1] and Gt[num_rows-1])");
+  return 0;
+}
+
+int effective_method(const dream_das_plan *p) { return p->Nr == 0 ? DREAM_DAS_SAFT : p->das_type; }
+
+int64_t terms_per_pixel(const dream_das_plan *p) {
+  return effective_method(p) == DREAM_DAS_SAFT ? p->Nt : p->Nt * p->Nr;
+}
+
+int64_t num_columns(const dream_das_plan *p) { return terms_per_pixel(p); }
+
+// Constants of DAS<double> / DAS<float> (extra_src/das.cc:316-318) and of the
+// das_uni float kernels (opencl/das_uni_float.cl:47-49).
+Consts64 constants_f64(double dt, double cp, double delay) {
+  Consts64 c;
+  c.Fs = (1.0 / dt) * 1000.0;
+  c.ocp = 1.0 / cp;
+  c.delay_ms = delay / 1000.0;
+  return c;
+}
+Consts32 constants_das_f32(float dt, float cp, float delay) {
+  Consts32 c;
+  c.Fs = (float)((1.0 / (double)dt) * 1000.0);
+  c.ocp = (float)(1.0 / (double)cp);
+  c.delay_ms = (float)((double)delay / 1000.0);
+  return c;
+}
+Consts32 constants_uni_f32(float dt, float cp, float delay) {
+  Consts32 c;
+  c.Fs = (1.0f / dt) * 1000.0f;
+  c.ocp = 1.0f / cp;
+  c.delay_ms = delay / 1000.0f;
+  return c;
+}
+
+// (int)((max - min)/d + 1.0) in the plan precision (include/das_uni.h:70-78).
+int64_t uni_count(double mn, double d, double mx, bool f32) {
+  double q;
+  if (f32) {
+    float qf = ((float)mx - (float)mn) / (float)d;
+    q = (double)qf + 1.0;
+  } else {
+    q = (mx - mn) / d + 1.0;
+  }
+  if (!(q >= 0.0) || q > 2147483647.0) return -1;
+  return (int64_t)(int)q;
+}
+
+int launch_plain(dream_das_plan *p, PlainLaunch &L, cudaStream_t st) {
+  // Pixel chunks keep a cancellation request observable between launches.
+  const int64_t tpp = std::max<int64_t>(terms_per_pixel(p), 1);
+  int64_t chunk = std::max<int64_t>(int64_t(1) << 16, (int64_t(1) << 33) / tpp);
+  chunk = (chunk + 255) / 256 * 256;
+  for (int64_t s = 0; s < L.No; s += chunk) {
+    if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
+    L.no0 = s;
+    L.no1 = std::min(L.No, s + chunk);
+    cudaError_t e = (p->precision == DREAM_PREC_F64) ? launch_plain_f64(L, st) : launch_plain_f32(L, st);
+    if (e != cudaSuccess) return cuda_fail(e, "DAS kernel launch");
+    p->launches++;
+  }
+  return 0;
+}
+
+// Fill a PlainLaunch for `das` (arbitrary geometry) on device pointers. The
+// delay (one value or No values) is read by the kernel from device memory and
+// converted to ms there, as DAS<T> does per pixel (extra_src/das.cc:131-136).
+int prepare_das(dream_das_plan *p, PlainLaunch &L, const void *dY, const void *dRo, const void *dGt,
+                const void *dGr, double dt, int delay_type, const void *ddelay, double cp, void *dIm,
+                unsigned long long *doob) {
+  memset(&L, 0, sizeof(L));
+  L.method = effective_method(p);
+  L.uni = false;
+  L.Y = dY;
+  L.K = p->K;
+  L.Ro = dRo;
+  L.No = p->No;
+  L.Gt = dGt;
+  L.Nt = p->Nt;
+  L.Gr = dGr;
+  L.Nr = (L.method == DREAM_DAS_SAFT) ? 0 : p->Nr;
+  L.Im = dIm;
+  L.oob = doob;
+  if (delay_type != DREAM_DELAY_SINGLE && delay_type != DREAM_DELAY_MULTIPLE)
+    return fail(DREAM_ERR_ARGUMENT, "unknown delay type");
+  if (ddelay == nullptr) return fail(DREAM_ERR_ARGUMENT, "delay pointer is NULL");
+  L.delay_vec = ddelay;
+  L.delay_multi = delay_type == DREAM_DELAY_MULTIPLE;
+  if (p->precision == DREAM_PREC_F64) L.c64 = constants_f64(dt, cp, 0.0);
+  else L.c32 = constants_das_f32((float)dt, (float)cp, 0.0f);
+  if (L.method >= DREAM_DAS_RCA_COLTX) {
+    int r = check_rca_edges(p->Nt, p->Nr);
+    if (r) return r;
+  }
+  if (p->No > 0 && (dRo == nullptr || dIm == nullptr)) return fail(DREAM_ERR_ARGUMENT, "NULL Ro or Im");
+  if (p->No > 0 && p->K > 0 && terms_per_pixel(p) > 0 && dY == nullptr)
+    return fail(DREAM_ERR_ARGUMENT, "NULL Y");
+  if (p->Nt > 0 && dGt == nullptr) return fail(DREAM_ERR_ARGUMENT, "NULL Gt");
+  if (L.Nr > 0 && dGr == nullptr) return fail(DREAM_ERR_ARGUMENT, "NULL Gr");
+  return 0;
+}
+
+__global__ void add_u64_kernel(unsigned long long *ctr, unsigned long long v) { *ctr += v; }
+
+// K == 0 (or no element pairs) has no in-bounds sample: the image is all
+// zeros and every term is out of bounds.
+int zero_length_ascans(dream_das_plan *p, void *dIm, unsigned long long *doob, cudaStream_t st) {
+  if (p->No > 0) CU(cudaMemsetAsync(dIm, 0, p->No * prec_size(p->precision), st));
+  unsigned long long oob = (unsigned long long)p->No * (unsigned long long)terms_per_pixel(p);
+  if (doob && oob) {
+    add_u64_kernel<<<1, 1, 0, st>>>(doob, oob);
+    CU(cudaGetLastError());
+    p->launches++;
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *dream_das_version(void) { return "dream_b200 das 0.1 (sm_100a)"; }
+
+const char *dream_das_last_error(void) { return g_last_error.c_str(); }
+
+int dream_das_plan_create(dream_das_plan **plan, int das_type, int64_t a_scan_len, int64_t No,
+                          int64_t num_t_elements, int64_t num_r_elements, int precision, int device) {
+  if (plan == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan pointer is NULL");
+  *plan = nullptr;
+  int r = check_common(das_type, a_scan_len, No, num_t_elements, num_r_elements, precision);
+  if (r) return r;
+  if (precision != DREAM_PREC_F64 && precision != DREAM_PREC_F32)
+    return fail(DREAM_ERR_UNSUPPORTED, "this plan kind supports F64 and F32 only");
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
+  if (device < 0 || device >= ndev) return fail(DREAM_ERR_ARGUMENT, "invalid CUDA device ordinal");
+  DeviceGuard g(device);
+  if (!g.ok) return fail(DREAM_ERR_CUDA, "cudaSetDevice failed");
+  dream_das_plan *p = new dream_das_plan();
+  p->das_type = das_type;
+  p->K = a_scan_len;
+  p->No = No;
+  p->Nt = num_t_elements;
+  p->Nr = (das_type == DREAM_DAS_SAFT) ? 0 : num_r_elements;
+  p->precision = precision;
+  p->device = device;
+  e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&p->h_oob, sizeof(unsigned long long));
+  if (e != cudaSuccess) {
+    dream_das_plan_destroy(p);
+    return cuda_fail(e, "plan setup");
+  }
+  r = p->bOob.ensure(sizeof(unsigned long long));
+  if (r) {
+    dream_das_plan_destroy(p);
+    return r;
+  }
+  *plan = p;
+  return 0;
+}
+
+int dream_das_setup_has_changed(const dream_das_plan *p, int das_type, int64_t a_scan_len, int64_t No,
+                                int64_t num_t_elements, int64_t num_r_elements, int precision, int device) {
+  if (p == nullptr) return 1;
+  int64_t nr = (das_type == DREAM_DAS_SAFT) ? 0 : num_r_elements;
+  return (p->uni || das_type != p->das_type || a_scan_len != p->K || No != p->No || num_t_elements != p->Nt ||
+          nr != p->Nr || precision != p->precision || device != p->device)
+             ? 1
+             : 0;
+}
+
+void dream_das_plan_destroy(dream_das_plan *p) {
+  if (p == nullptr) return;
+  {
+    DeviceGuard g(p->device);
+    if (p->stream) cudaStreamSynchronize(p->stream);
+    p->bY.release();
+    p->bRo.release();
+    p->bGt.release();
+    p->bGr.release();
+    p->bDelay.release();
+    p->bIm.release();
+    p->bOob.release();
+    if (p->h_oob) cudaFreeHost(p->h_oob);
+    if (p->stream) cudaStreamDestroy(p->stream);
+  }
+  delete p;
+}
+
+void dream_das_cancel(dream_das_plan *p) {
+  if (p) p->cancelled.store(true);
+}
+
+void dream_das_set_running(dream_das_plan *p) {
+  if (p) p->cancelled.store(false);
+}
+
+int64_t dream_das_plan_num_points(const dream_das_plan *p) { return p ? p->No : -1; }
+
+int64_t dream_das_plan_num_ascans(const dream_das_plan *p) { return p ? num_columns(p) : -1; }
+
+int64_t dream_das_plan_launch_count(const dream_das_plan *p) { return p ? p->launches.load() : -1; }
+
+static int run_device_impl(dream_das_plan *p, const void *dY, const void *dRo, const void *dGt, const void *dGr,
+                           double dt, int delay_type, const void *ddelay, double cp, void *dIm,
+                           unsigned long long *doob, cudaStream_t st) {
+  PlainLaunch L;
+  int r = prepare_das(p, L, dY, dRo, dGt, dGr, dt, delay_type, ddelay, cp, dIm, doob);
+  if (r) return r;
+  if (p->No == 0) return 0;
+  if (p->K == 0 || terms_per_pixel(p) == 0) return zero_length_ascans(p, dIm, doob, st);
+  return launch_plain(p, L, st);
+}
+
+int dream_das_run_device(dream_das_plan *p, const void *dY, const void *dRo, const void *dGt, const void *dGr,
+                         double dt, int delay_type, const void *ddelay, double cp, void *dIm, int err_level,
+                         int64_t *oob_count, void *stream) {
+  if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
+  if (p->uni) return fail(DREAM_ERR_ARGUMENT, "uniform-grid plan passed to dream_das_run_device");
+  if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  cudaStream_t st = (cudaStream_t)stream;  // NULL: the default stream
+  unsigned long long *doob = (unsigned long long *)p->bOob.p;
+  CU(cudaMemsetAsync(doob, 0, sizeof(unsigned long long), st));
+  int r = run_device_impl(p, dY, dRo, dGt, dGr, dt, delay_type, ddelay, cp, dIm, doob, st);
+  if (r) return r;
+  CU(cudaMemcpyAsync(p->h_oob, doob, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  uint64_t oob = *p->h_oob;
+  if (oob_count) *oob_count = (int64_t)oob;
+  return status_from_oob(oob, err_level);
+}
+
+int dream_das_run_device_async(dream_das_plan *p, const void *dY, const void *dRo, const void *dGt,
+                               const void *dGr, double dt, int delay_type, const void *ddelay, double cp,
+                               void *dIm, unsigned long long *d_oob, void *stream) {
+  if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
+  if (p->uni) return fail(DREAM_ERR_ARGUMENT, "uniform-grid plan passed to dream_das_run_device_async");
+  if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  cudaStream_t st = (cudaStream_t)stream;  // NULL: the default stream
+  return run_device_impl(p, dY, dRo, dGt, dGr, dt, delay_type, ddelay, cp, dIm, d_oob, st);
+}
+
+int dream_das_run(dream_das_plan *p, const void *Y, const void *Ro, const void *Gt, const void *Gr, double dt,
+                  int delay_type, const void *delay, double cp, void *Im, int err_level, int64_t *oob_count) {
+  if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
+  if (p->uni) return fail(DREAM_ERR_ARGUMENT, "uniform-grid plan passed to dream_das_run");
+  if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
+  if (delay == nullptr) return fail(DREAM_ERR_ARGUMENT, "delay pointer is NULL");
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  cudaStream_t st = p->stream;
+  const size_t es = prec_size(p->precision);
+  const int method = effective_method(p);
+  const int64_t ncol = num_columns(p);
+  const int64_t nr = (method == DREAM_DAS_SAFT) ? 0 : p->Nr;
+  const bool multi = delay_type == DREAM_DELAY_MULTIPLE && p->No != 1;
+  int r;
+  if ((r = p->bY.ensure((size_t)p->K * ncol * es))) return r;
+  if ((r = p->bRo.ensure((size_t)p->No * 3 * es))) return r;
+  if ((r = p->bGt.ensure((size_t)p->Nt * 3 * es))) return r;
+  if ((r = p->bGr.ensure((size_t)nr * 3 * es))) return r;
+  if ((r = p->bDelay.ensure((size_t)(multi ? p->No : 1) * es))) return r;
+  if ((r = p->bIm.ensure((size_t)p->No * es))) return r;
+  if (p->K * ncol > 0) CU(cudaMemcpyAsync(p->bY.p, Y, (size_t)p->K * ncol * es, cudaMemcpyHostToDevice, st));
+  if (p->No > 0) CU(cudaMemcpyAsync(p->bRo.p, Ro, (size_t)p->No * 3 * es, cudaMemcpyHostToDevice, st));
+  if (p->Nt > 0) CU(cudaMemcpyAsync(p->bGt.p, Gt, (size_t)p->Nt * 3 * es, cudaMemcpyHostToDevice, st));
+  if (nr > 0) CU(cudaMemcpyAsync(p->bGr.p, Gr, (size_t)nr * 3 * es, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(p->bDelay.p, delay, (size_t)(multi ? p->No : 1) * es, cudaMemcpyHostToDevice, st));
+  unsigned long long *doob = (unsigned long long *)p->bOob.p;
+  CU(cudaMemsetAsync(doob, 0, sizeof(unsigned long long), st));
+  r = run_device_impl(p, p->bY.p, p->bRo.p, p->bGt.p, p->bGr.p, dt, delay_type, p->bDelay.p, cp, p->bIm.p,
+                      doob, st);
+  if (r) return r;
+  if (p->No > 0) CU(cudaMemcpyAsync(Im, p->bIm.p, (size_t)p->No * es, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(p->h_oob, doob, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  uint64_t oob = *p->h_oob;
+  if (oob_count) *oob_count = (int64_t)oob;
+  return status_from_oob(oob, err_level);
+}
+
+// ---------------------------------------------------------------------------
+// das_uni
+// ---------------------------------------------------------------------------
+
+int dream_das_uni_plan_create(dream_das_plan **plan, int das_type, int64_t a_scan_len, const double *tri,
+                              int precision, int device) {
+  if (plan == nullptr || tri == nullptr) return fail(DREAM_ERR_ARGUMENT, "NULL argument");
+  *plan = nullptr;
+  if (precision != DREAM_PREC_F64 && precision != DREAM_PREC_F32)
+    return fail(DREAM_ERR_UNSUPPORTED, "das_uni supports F64 and F32");
+  const bool f32 = precision == DREAM_PREC_F32;
+  int64_t Nt = uni_count(tri[0], tri[1], tri[2], f32);
+  int64_t Nr = (das_type == DREAM_DAS_SAFT) ? 0 : uni_count(tri[3], tri[4], tri[5], f32);
+  int64_t Nx = uni_count(tri[6], tri[7], tri[8], f32);
+  int64_t Ny = uni_count(tri[9], tri[10], tri[11], f32);
+  int64_t Nz = uni_count(tri[12], tri[13], tri[14], f32);
+  if (Nt < 0 || Nr < 0 || Nx < 0 || Ny < 0 || Nz < 0)
+    return fail(DREAM_ERR_ARGUMENT, "invalid (min, pitch, max) triplet");
+  if (Nx * Ny * Nz > ((int64_t)1 << 40)) return fail(DREAM_ERR_ARGUMENT, "too many image points");
+  if (das_type != DREAM_DAS_SAFT && Nr == 0) return fail(DREAM_ERR_ARGUMENT, "empty receive triplet");
+  int r = dream_das_plan_create(plan, das_type, a_scan_len, Nx * Ny * Nz, Nt, Nr, precision, device);
+  if (r) return r;
+  dream_das_plan *p = *plan;
+  p->uni = true;
+  for (int i = 0; i < 15; i++) p->tri[i] = tri[i];
+  p->Nx = Nx;
+  p->Ny = Ny;
+  p->Nz = Nz;
+  return 0;
+}
+
+static int uni_launch(dream_das_plan *p, const void *dY, const double *tri, double dt, double delay, double cp,
+                      void *dIm, unsigned long long *doob, cudaStream_t st) {
+  for (int i = 0; i < 15; i++) {
+    if (p->das_type == DREAM_DAS_SAFT && i >= 3 && i < 6) continue;
+    if (tri[i] != p->tri[i] && !(tri[i] != tri[i] && p->tri[i] != p->tri[i]))
+      return fail(DREAM_ERR_ARGUMENT, "triplets differ from the plan's (create a new plan)");
+  }
+  PlainLaunch L;
+  memset(&L, 0, sizeof(L));
+  L.method = effective_method(p);
+  L.uni = true;
+  L.Y = dY;
+  L.K = p->K;
+  L.No = p->No;
+  L.Nt = p->Nt;
+  L.Nr = p->Nr;
+  L.Nx = p->Nx;
+  L.Ny = p->Ny;
+  L.Nz = p->Nz;
+  L.Im = dIm;
+  L.oob = doob;
+  for (int i = 0; i < 15; i++) {
+    L.tri64[i] = tri[i];
+    L.tri32[i] = (float)tri[i];
+  }
+  if (p->precision == DREAM_PREC_F64) L.c64 = constants_f64(dt, cp, delay);
+  else L.c32 = constants_uni_f32((float)dt, (float)cp, (float)delay);
+  if (p->No == 0) return 0;
+  if (p->K == 0) return zero_length_ascans(p, dIm, doob, st);
+  return launch_plain(p, L, st);
+}
+
+int dream_das_uni_run_device(dream_das_plan *p, const void *dY, const double *tri, double dt, double delay,
+                             double cp, void *dIm, int err_level, int64_t *oob_count, void *stream) {
+  if (p == nullptr || !p->uni) return fail(DREAM_ERR_ARGUMENT, "not a uniform-grid plan");
+  if (tri == nullptr) return fail(DREAM_ERR_ARGUMENT, "tri is NULL");
+  if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  cudaStream_t st = (cudaStream_t)stream;  // NULL: the default stream
+  unsigned long long *doob = (unsigned long long *)p->bOob.p;
+  CU(cudaMemsetAsync(doob, 0, sizeof(unsigned long long), st));
+  int r = uni_launch(p, dY, tri, dt, delay, cp, dIm, doob, st);
+  if (r) return r;
+  CU(cudaMemcpyAsync(p->h_oob, doob, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  uint64_t oob = *p->h_oob;
+  if (oob_count) *oob_count = (int64_t)oob;
+  return status_from_oob(oob, err_level);
+}
+
+int dream_das_uni_run(dream_das_plan *p, const void *Y, const double *tri, double dt, double delay, double cp,
+                      void *Im, int err_level, int64_t *oob_count) {
+  if (p == nullptr || !p->uni) return fail(DREAM_ERR_ARGUMENT, "not a uniform-grid plan");
+  if (tri == nullptr) return fail(DREAM_ERR_ARGUMENT, "tri is NULL");
+  if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  cudaStream_t st = p->stream;
+  const size_t es = prec_size(p->precision);
+  const int64_t ncol = num_columns(p);
+  int r;
+  if ((r = p->bY.ensure((size_t)p->K * ncol * es))) return r;
+  if ((r = p->bIm.ensure((size_t)p->No * es))) return r;
+  if (p->K * ncol > 0) CU(cudaMemcpyAsync(p->bY.p, Y, (size_t)p->K * ncol * es, cudaMemcpyHostToDevice, st));
+  unsigned long long *doob = (unsigned long long *)p->bOob.p;
+  CU(cudaMemsetAsync(doob, 0, sizeof(unsigned long long), st));
+  r = uni_launch(p, p->bY.p, tri, dt, delay, cp, p->bIm.p, doob, st);
+  if (r) return r;
+  if (p->No > 0) CU(cudaMemcpyAsync(Im, p->bIm.p, (size_t)p->No * es, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(p->h_oob, doob, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  uint64_t oob = *p->h_oob;
+  if (oob_count) *oob_count = (int64_t)oob;
+  return status_from_oob(oob, err_level);
+}
+
+}  // extern "C"

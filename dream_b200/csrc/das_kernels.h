@@ -1,0 +1,45 @@
+// das_kernels.h -- launch descriptors shared by the C ABI (das_capi.cu) and
+// the kernel translation units. Host-side only types.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dream {
+
+// Per-call constants, computed on the host exactly as the restated reference
+// source computes them (see das_capi.cu: constants_*).
+struct Consts64 {
+  double Fs, ocp, delay_ms;
+};
+struct Consts32 {
+  float Fs, ocp, delay_ms;
+};
+
+struct PlainLaunch {
+  int method;  // 0 SAFT, 1 TFM, 2 RCA col-tx, 3 RCA row-tx
+  bool uni;
+  const void *Y;
+  int64_t K;
+  const void *Ro;
+  int64_t No;
+  int64_t no0, no1;  // pixel range of this launch
+  const void *Gt;
+  int64_t Nt;
+  const void *Gr;
+  int64_t Nr;
+  const void *delay_vec;  // device delays (us): 1 value, or No values when delay_multi
+  bool delay_multi;
+  Consts64 c64;
+  Consts32 c32;
+  double tri64[15];
+  float tri32[15];
+  int64_t Nx, Ny, Nz;
+  void *Im;
+  unsigned long long *oob;
+};
+
+cudaError_t launch_plain_f64(const PlainLaunch &L, cudaStream_t st);
+cudaError_t launch_plain_f32(const PlainLaunch &L, cudaStream_t st);
+
+}  // namespace dream

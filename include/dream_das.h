@@ -1,0 +1,182 @@
+/*
+ * dream_das.h -- C ABI of the B200 (sm_100a) delay-and-sum beamformer.
+ *
+ * This is the drop-in boundary for DREAM's DAS path. Every entry point takes
+ * plain pointers and sizes; array layouts are DREAM's (column-major):
+ *   Y   [K x C]   A-scans, sample k of A-scan column c at Y[k + c*K]
+ *               (C = Nt for SAFT, Nt*Nr for TFM and RCA col-tx, Nr*Nt for
+ *                RCA row-tx, exactly the reference's column order)
+ *   Ro  [No x 3]  observation points, Ro[n + j*No]
+ *   Gt  [Nt x 3]  transmit elements (RCA: the columns), Gt[n + j*Nt]
+ *   Gr  [Nr x 3]  receive elements (RCA: the rows)
+ *   delay         1 value or No values [us]; dt [us]; cp [m/s]; positions [mm]
+ *   Im  [No]      output image
+ *
+ * Reference interfaces replaced (paths inside the DREAM source tree):
+ *   dream_das_plan_create        DAS<T>::DAS (include/das.h:56-63,
+ *                                extra_src/das.cc:36-53; OpenCL ctor
+ *                                opencl/cl_das.cc:30-52)
+ *   dream_das_setup_has_changed  DAS<T>::das_setup_has_changed (include/das.h:77-94)
+ *   dream_das_run                DAS<T>::das (include/das.h:67-72,
+ *                                extra_src/das.cc:199-298) and
+ *                                DAS<T>::cl_das (opencl/cl_das.cc:61-159)
+ *   dream_das_uni_plan_create    DAS_UNI<T>::DAS_UNI (include/das_uni.h:55-64,
+ *                                opencl/cl_das_uni.cc:32-60)
+ *   dream_das_uni_run            DAS_UNI<T>::cl_das_uni (opencl/cl_das_uni.cc:70-187)
+ *   dream_das_cancel             DAS<T>::abort (extra_src/das.cc:61-65)
+ *   status values                SIRError (include/dream.h:42-47)
+ *   err_level values             ErrorLevel (include/dream.h:49-55)
+ *   das_type values              DASType (include/dream.h:97-102)
+ *   delay_type values            DelayType (include/dream.h:57-60)
+ *
+ * Thread safety: no globals are shared between plans; use one plan per host
+ * thread (or per stream). A plan serialises its own calls.
+ */
+#ifndef DREAM_DAS_H
+#define DREAM_DAS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes: >= 0 mirror SIRError, < 0 are errors of this library ---- */
+#define DREAM_STATUS_NONE 0
+#define DREAM_STATUS_IGNORE_OUT_OF_BOUNDS 1
+#define DREAM_STATUS_WARN_OUT_OF_BOUNDS 2
+#define DREAM_STATUS_OUT_OF_BOUNDS 3
+#define DREAM_ERR_ARGUMENT (-1)    /* invalid argument or shape */
+#define DREAM_ERR_CUDA (-2)        /* CUDA runtime error (message via dream_das_last_error) */
+#define DREAM_ERR_ALLOC (-3)       /* device allocation failed */
+#define DREAM_ERR_UNSUPPORTED (-4) /* combination not implemented */
+#define DREAM_ERR_CANCELLED (-5)   /* dream_das_cancel was called */
+
+/* ---- enums (values equal the reference's enum class ordinals) ---- */
+#define DREAM_DAS_SAFT 0
+#define DREAM_DAS_TFM 1
+#define DREAM_DAS_RCA_COLTX 2
+#define DREAM_DAS_RCA_ROWTX 3
+
+#define DREAM_ERR_LEVEL_NONE 0
+#define DREAM_ERR_LEVEL_IGNORE 1
+#define DREAM_ERR_LEVEL_WARN 2
+#define DREAM_ERR_LEVEL_STOP 3
+#define DREAM_ERR_LEVEL_PARALLEL_STOP 4
+
+#define DREAM_DELAY_SINGLE 0
+#define DREAM_DELAY_MULTIPLE 1
+
+/*
+ * Precision of a plan.
+ *   F64   DAS<double>: everything in FP64; sample indices and images are
+ *         bit-identical to the reference CPU `das`.
+ *   F32   DAS<float>: everything in FP32 with the reference's constants;
+ *         indices and images bit-identical to the reference `das_f`.
+ *   F32_STORE  geometry in FP64 and FP64-exact sample indices (the indices
+ *         of F64), A-scans stored in FP32, FP32 compensated accumulation,
+ *         FP32 image.
+ *   BF16_STORE as F32_STORE with the A-scans stored in BF16 (the plan
+ *         converts FP32 input on the device; device-pointer calls may pass
+ *         BF16 directly, see dream_das_run_device).
+ */
+#define DREAM_PREC_F64 0
+#define DREAM_PREC_F32 1
+#define DREAM_PREC_F32_STORE 2
+#define DREAM_PREC_BF16_STORE 3
+
+typedef struct dream_das_plan dream_das_plan;
+
+/* Library version string. */
+const char *dream_das_version(void);
+
+/* Message of the last error raised on this host thread ("" if none). */
+const char *dream_das_last_error(void);
+
+/*
+ * Creates a plan (the persistent object the reference bindings cache).
+ * num_r_elements == 0 selects SAFT whatever das_type says
+ * (extra_src/das.cc:211-213). device is the CUDA ordinal.
+ */
+int dream_das_plan_create(dream_das_plan **plan, int das_type, int64_t a_scan_len, int64_t No,
+                          int64_t num_t_elements, int64_t num_r_elements, int precision,
+                          int device);
+
+/* 1 if a plan cannot be reused for this setup, 0 if it can. */
+int dream_das_setup_has_changed(const dream_das_plan *plan, int das_type, int64_t a_scan_len,
+                                int64_t No, int64_t num_t_elements, int64_t num_r_elements,
+                                int precision, int device);
+
+void dream_das_plan_destroy(dream_das_plan *plan);
+
+/*
+ * Runs DAS on HOST buffers (copies in, computes, copies out; blocking).
+ * Element types: F64 -> double for all arrays; F32 -> float for all arrays;
+ * F32_STORE / BF16_STORE -> Y float, Ro/Gt/Gr/delay double, Im float.
+ * dt, cp are passed as double; F32 plans round them to float first, as a
+ * float-typed caller of DAS<float> would have them.
+ * Returns a status (see above); oob_count (may be NULL) receives the number
+ * of out-of-bounds terms.
+ */
+int dream_das_run(dream_das_plan *plan, const void *Y, const void *Ro, const void *Gt,
+                  const void *Gr, double dt, int delay_type, const void *delay, double cp,
+                  void *Im, int err_level, int64_t *oob_count);
+
+/*
+ * As dream_das_run on DEVICE buffers, enqueued on `stream` (a cudaStream_t;
+ * NULL is the default stream). Waits for the stream to report the status.
+ * BF16_STORE plans take Y as BF16 (uint16 bit patterns) here.
+ */
+int dream_das_run_device(dream_das_plan *plan, const void *dY, const void *dRo, const void *dGt,
+                         const void *dGr, double dt, int delay_type, const void *ddelay, double cp,
+                         void *dIm, int err_level, int64_t *oob_count, void *stream);
+
+/*
+ * Fully asynchronous device variant: never synchronises and adds the number
+ * of out-of-bounds terms to the caller's device counter d_oob (uint64, may be
+ * NULL). Safe to capture in a CUDA graph. Returns only argument errors.
+ */
+int dream_das_run_device_async(dream_das_plan *plan, const void *dY, const void *dRo,
+                               const void *dGt, const void *dGr, double dt, int delay_type,
+                               const void *ddelay, double cp, void *dIm,
+                               unsigned long long *d_oob, void *stream);
+
+/*
+ * Uniform-grid plan (DAS_UNI). tri holds 15 values:
+ *   [min_t, pitch_t, max_t, min_r, pitch_r, max_r,
+ *    min_x, dx, max_x, min_y, dy, max_y, min_z, dz, max_z]
+ * (the receive triplet is ignored for SAFT). Only F64 and F32 are offered.
+ * Counts are (int)((max - min)/pitch + 1.0) in the plan precision
+ * (include/das_uni.h:70-78); pixel n maps to (ny fastest, then nz, then nx).
+ */
+int dream_das_uni_plan_create(dream_das_plan **plan, int das_type, int64_t a_scan_len,
+                              const double *tri, int precision, int device);
+
+/* Number of image points of a plan (uniform plans: Nx*Ny*Nz). */
+int64_t dream_das_plan_num_points(const dream_das_plan *plan);
+
+/* Number of A-scan columns Y must hold (Nt for SAFT, Nt*Nr otherwise). */
+int64_t dream_das_plan_num_ascans(const dream_das_plan *plan);
+
+/* Runs das_uni on host buffers: Y (T), Im (T) with T of the plan precision. */
+int dream_das_uni_run(dream_das_plan *plan, const void *Y, const double *tri, double dt,
+                      double delay, double cp, void *Im, int err_level, int64_t *oob_count);
+
+/* Device-buffer variant of dream_das_uni_run. */
+int dream_das_uni_run_device(dream_das_plan *plan, const void *dY, const double *tri, double dt,
+                             double delay, double cp, void *dIm, int err_level,
+                             int64_t *oob_count, void *stream);
+
+/* Number of kernels this plan has launched since it was created. */
+int64_t dream_das_plan_launch_count(const dream_das_plan *plan);
+
+/* Requests cancellation: running and later calls return DREAM_ERR_CANCELLED
+ * between launches until dream_das_set_running is called. */
+void dream_das_cancel(dream_das_plan *plan);
+void dream_das_set_running(dream_das_plan *plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DREAM_DAS_H */

@@ -153,7 +153,7 @@ static int oob_status(int err_level)
 #define TERM(t_dp, term)                                                                  \
   {                                                                                       \
     T p_ = (t_dp) * Fs_khz;                                                               \
-    int in_ = (p_ > (T)-1.0) && (p_ < (T)K);                                              \
+    int in_ = (K > 0) && (p_ > (T)-1.0) && (p_ < (T)K);                                   \
     int64_t k_ = in_ ? (int64_t)p_ : INT64_MIN;                                           \
     if (idx_out) idx_out[(int64_t)(term) * No + no] = k_;                                 \
     if (in_) {                                                                            \
@@ -165,8 +165,8 @@ static int oob_status(int err_level)
     }                                                                                     \
   }
 
-/* The bounds test (p > -1) && (p < K) equals (trunc(p) >= 0) && (trunc(p) < K)
- * for integer K, and leaves NaN out of bounds, which is where the reference's
+/* For K >= 1 the bounds test (p > -1) && (p < K) equals (trunc(p) >= 0) &&
+ * (trunc(p) < K) for integer K (K == 0 has no in-bounds sample), and leaves NaN out of bounds, which is where the reference's
  * integer conversion of NaN (INT64_MIN on x86-64) also lands. */
 
 #define DELAY_MS(d) ((double)(d) / 1000.0)
@@ -321,7 +321,7 @@ int64_t dream_oracle_uni_count_f32(float mn, float d, float mx)
 #define UTERM(t_dp)                                                                       \
   {                                                                                       \
     T p_ = (t_dp) * Fs_khz;                                                               \
-    if ((p_ > (T)-1.0) && (p_ < (T)K)) {                                                  \
+    if ((K > 0) && (p_ > (T)-1.0) && (p_ < (T)K)) {                                       \
       im += y_p[(int64_t)p_];                                                             \
     } else {                                                                              \
       int s_ = oob_status(err_level);                                                     \
