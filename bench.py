@@ -13,7 +13,7 @@ data-path collective). One JSON line is printed by rank 0.
 
 value : whole-job Gsum/s with inputs resident in HBM (CUDA events on the
         launching stream, L2 flushed between steps by writing 256 MiB).
-e2e   : the same metric through the public API (dream_b200.das_f.das) from
+e2e   : the same metric through the public API (dream_b200.beamformer.das_mixed) from
         pinned host arrays: H2D of the inputs and D2H of the image each step.
 """
 from __future__ import annotations
@@ -239,21 +239,31 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     d_oob = torch.zeros(1, dtype=torch.int64, device=dev)
+    from dream_b200.beamformer import grid_hint
+    hint = grid_hint(scene.Ro)
 
-    def variant(prec_code, np_dt, steps, warmup):
-        Y, Gt, Gr, Ro = (dev_f(a, np_dt) for a in (s32.Y if np_dt == np.float32 else scene.Y, scene.Gt,
-                                                     scene.Gr, scene.Ro))
-        delay = dev_f(np.zeros((1, 1)), np_dt)
-        Im = torch.empty(No, dtype=Y.dtype, device=dev)
+    def variant(prec_code, steps, warmup):
+        geo_dt = np.float32 if prec_code == _lib.PREC_F32 else np.float64
+        y_dt = np.float64 if prec_code == _lib.PREC_F64 else np.float32
+        Y = dev_f(scene.Y, y_dt)
+        if prec_code == _lib.PREC_BF16_STORE:
+            Y = Y.t().contiguous().to(torch.bfloat16).t()
+        Gt, Gr, Ro = (dev_f(a, geo_dt) for a in (scene.Gt, scene.Gr, scene.Ro))
+        delay = dev_f(np.zeros((1, 1)), geo_dt)
+        Im = torch.empty(No, dtype=torch.float64 if prec_code == _lib.PREC_F64 else torch.float32, device=dev)
         plan = _lib.plan_create(_lib.TFM, K, No, Nt, Nr, prec_code, local)
+        if prec_code in (_lib.PREC_F32_STORE, _lib.PREC_BF16_STORE):
+            _lib.check(L.dream_das_set_grid_hint(plan.handle, hint))
         ptr = lambda t: ctypes.c_void_p(t.data_ptr())
-        args_ = (plan.handle, ptr(Y), ptr(Ro), ptr(Gt), ptr(Gr), float(np_dt(scene.dt)), _lib.DELAY_SINGLE,
-                 ptr(delay), float(np_dt(scene.cp)), ptr(Im), ctypes.c_void_p(d_oob.data_ptr()),
+        cast = (lambda v: float(np.float32(v))) if prec_code == _lib.PREC_F32 else float
+        args_ = (plan.handle, ptr(Y), ptr(Ro), ptr(Gt), ptr(Gr), cast(scene.dt), _lib.DELAY_SINGLE,
+                 ptr(delay), cast(scene.cp), ptr(Im), ctypes.c_void_p(d_oob.data_ptr()),
                  ctypes.c_void_p(stream.cuda_stream))
 
         def launch():
             _lib.check(L.dream_das_run_device_async(*args_))
 
+        d_oob.zero_()
         for _ in range(warmup):
             flush.fill_(1.0)
             launch()
@@ -264,7 +274,7 @@ def main():
         n0 = L.dream_das_plan_launch_count(plan.handle)
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
         for i in range(steps):
-            flush.fill_(float(i))  # 256 MiB write: evicts Y (49 MB FP32) from the 126 MB L2
+            flush.fill_(float(i))  # 256 MiB write evicts the A-scans (49-98 MB) from the 126 MB L2
             evs[i][0].record(stream)
             launch()
             evs[i][1].record(stream)
@@ -279,18 +289,21 @@ def main():
             dist.all_reduce(tot, op=dist.ReduceOp.MAX)
         if int(d_oob.item()) != 0:
             raise RuntimeError("unexpected out-of-bounds terms in the benchmark scene")
-        return float(tot.item()), ms, launches, Im
+        return float(tot.item()), launches, Im
 
     clocks = ClockSampler(local)
     clocks.start()
-    tot32, ms32, launches32, Im32 = variant(_lib.PREC_F32, np.float32, args.steps, args.warmup)
+    tot_h, launches_h, Im_h = variant(_lib.PREC_F32_STORE, args.steps, args.warmup)
     clk = clocks.stop()
-    f64_steps = max(3, args.steps // 4)
-    tot64, ms64, launches64, _ = variant(_lib.PREC_F64, np.float64, f64_steps, max(3, args.warmup // 2))
+    side = max(3, args.steps // 4)
+    others = {}
+    for name, code in (("bf16_store", _lib.PREC_BF16_STORE), ("plain_f32", _lib.PREC_F32),
+                       ("plain_f64", _lib.PREC_F64)):
+        t, _, _ = variant(code, side, max(3, args.warmup // 2))
+        others[name] = {"gsum_s": world * sums / (t / side * 1e-3) / 1e9, "ms_per_frame": t / side}
 
-    step_ms = tot32 / args.steps
+    step_ms = tot_h / args.steps
     value = world * sums / (step_ms * 1e-3) / 1e9
-    value64 = world * sums / (tot64 / f64_steps * 1e-3) / 1e9
 
     # ---- e2e through the public API from pinned host memory ----
     def pinned_f(a, dt):
@@ -301,18 +314,23 @@ def main():
         arr[...] = a
         return arr
 
-    hY, hGt, hGr, hRo = (pinned_f(a, np.float32) for a in (s32.Y, s32.Gt, s32.Gr, s32.Ro))
-    hdelay = pinned_f(np.zeros((1, 1)), np.float32)
+    from dream_b200.beamformer import das_mixed
+    hY = pinned_f(scene.Y, np.float32)
+    hGt, hGr, hRo = (pinned_f(a, np.float64) for a in (scene.Gt, scene.Gr, scene.Ro))
+    hdelay = pinned_f(np.zeros((1, 1)), np.float64)
     e2e_steps = max(3, args.steps // 2)
+
+    def e2e_call():
+        return das_mixed(hY, hGt, hGr, hRo, scene.dt, hdelay, scene.cp, "tfm", "ignore", "cuda", "f32")
+
     for _ in range(2):
-        das_f.das(hY, hGt, hGr, hRo, np.float32(s32.dt), hdelay, np.float32(s32.cp), "tfm", "ignore", "cuda")
+        e2e_call()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        out = das_f.das(hY, hGt, hGr, hRo, np.float32(s32.dt), hdelay, np.float32(s32.cp), "tfm", "ignore",
-                        "cuda")
+        out = e2e_call()
     t_e2e = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
@@ -335,22 +353,19 @@ def main():
         "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded point scatterers, Gaussian-windowed 5 MHz sine, N(0,0.01) noise)",
         "config": {"workload": WORKLOAD, "global_batch": world, "frames_per_gpu": 1,
-                   "precision": "plain FP32 (bit-exact with reference das_f)",
+                   "precision": "FP32-stored A-scans, FP32 compensated sums, FP64-exact sample indices",
                    "l2": "flushed between timed steps (256 MiB write, outside the timed events)",
                    "parallelism": f"{world} independent frames, one per GPU"},
-        "variants": {
-            "plain_f32": {"gsum_s": value, "ms_per_frame": step_ms},
-            "plain_f64": {"gsum_s": value64, "ms_per_frame": tot64 / f64_steps},
-        },
+        "variants": dict({"f32_store": {"gsum_s": value, "ms_per_frame": step_ms}}, **others),
         "e2e": {"value": e2e_val, "unit": "Gsum/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "api": "dream_b200.das_f.das(numpy arrays in pinned host memory, device='cuda')"},
+                "api": "dream_b200.beamformer.das_mixed(pinned host arrays, device='cuda', storage='f32')"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": read_traffic("das_plain_f32_tfm"),
+                     "traffic": read_traffic("das_fast_f32_tfm"),
                      "peak_source": f"{peak_kind} hbm_gbs",
                      "algorithmic_bytes_per_launch": gathered,
                      "note": "achieved = gathered sample bytes (4 B per sum) / kernel time",
                      "compulsory_hbm_frac": compulsory / (step_ms * 1e-3) / 1e9 / peak},
-        "gpu_launches": int(launches32),
+        "gpu_launches": int(launches_h),
         "clocks": clk,
     }
     if not args.no_cpu_baseline:

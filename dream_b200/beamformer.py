@@ -250,3 +250,94 @@ def das_uni(Y, gt, gr, ro, dt, delay, cp, method, err_level="ignore", device="cu
                                             ctypes.byref(oob)))
     _report(st, "DAS_UNI")
     return Im
+
+
+# ---------------------------------------------------------------------------
+# Precision upgrade: FP32/BF16-stored A-scans, FP32 compensated sums, FP64-exact
+# sample indices. Not part of the reference surface; same arguments plus
+# `storage` and optional per-A-scan weights.
+# ---------------------------------------------------------------------------
+
+_STORAGE = {"f32": _lib.PREC_F32_STORE, "bf16": _lib.PREC_BF16_STORE}
+
+
+def grid_hint(Ro) -> int:
+    """Number of leading image points that share x and y (the fastest grid
+    axis, e.g. Nz for ``meshgrid(x, z)`` flattened column-major), or 0 when
+    it does not divide the number of points."""
+    No = int(Ro.shape[0])
+    if No == 0:
+        return 0
+    if _is_torch(Ro):
+        import torch
+        ch = torch.nonzero((Ro[:, 0] != Ro[0, 0]) | (Ro[:, 1] != Ro[0, 1]))
+        n = int(ch[0, 0].item()) if ch.numel() else No
+    else:
+        R = np.asarray(Ro)
+        ch = np.nonzero((R[:, 0] != R[0, 0]) | (R[:, 1] != R[0, 1]))[0]
+        n = int(ch[0]) if ch.size else No
+    return n if (n > 0 and No % n == 0 and n < No) else 0
+
+
+def _fast_plan(das_type, K, No, Nt, Nr, prec, dev, hint, tile=None):
+    key = ("fast", das_type, K, No, Nt, Nr, prec, dev)
+    plan = _plan(key, lambda: _lib.plan_create(das_type, K, No, Nt, Nr, prec, dev))
+    L = _lib.load()
+    if getattr(plan, "hint", None) != hint:
+        _lib.check(L.dream_das_set_grid_hint(plan.handle, int(hint)))
+        plan.hint = hint
+        plan.tile = None
+    if tile is not None and getattr(plan, "tile", None) != tuple(tile):
+        _lib.check(L.dream_das_set_tile(plan.handle, int(tile[0]), int(tile[1])))
+        plan.tile = tuple(tile)
+    return plan
+
+
+def das_mixed(Y, Gt, Gr, Ro, dt, delay, cp, method, err_level="stop", device="cuda", storage="f32",
+              weights=None, hint="auto", tile=None, stream=None):
+    """DAS with A-scans stored in FP32 (``storage='f32'``) or BF16 and FP32
+    compensated accumulation; sample indices are the FP64 reference's.
+
+    Geometry and delays are taken in FP64. Returns an FP32 image (a torch
+    tensor on the device when Y is a CUDA tensor, else a NumPy array).
+    ``weights`` (one per A-scan column) gives ``sum_c w[c] * Y[k, c]``.
+    """
+    import torch
+    das_type = parse_method(method)
+    level = parse_err_level(err_level)
+    dev = parse_device(device)
+    prec = _STORAGE[storage]
+    on_host = not (_is_torch(Y) and Y.device.type == "cuda")
+    device_t = Y.device if not on_host else torch.device("cuda", dev)
+    dev = device_t.index if device_t.index is not None else torch.cuda.current_device()
+    ydt = np.float32
+    Yt = _torch_fortran(Y, ydt, device_t)
+    if prec == _lib.PREC_BF16_STORE:
+        Yt = Yt.t().contiguous().to(torch.bfloat16).t()
+    Gt_t = _torch_fortran(Gt, np.float64, device_t)
+    Gr_t = _torch_fortran(Gr, np.float64, device_t) if Gr is not None and das_type != _lib.SAFT else None
+    Ro_t = _torch_fortran(Ro, np.float64, device_t)
+    dl_t = _torch_fortran(delay, np.float64, device_t)
+    K, No, Nt, Nr, multi = _check_shapes(Yt, Gt_t, Gr_t, Ro_t, dl_t, das_type)
+    h = grid_hint(Ro if not on_host else np.asarray(Ro)) if hint == "auto" else int(hint or 0)
+    plan = _fast_plan(das_type, K, No, Nt, Nr, prec, dev, h, tile)
+    Im = torch.empty(No, dtype=torch.float32, device=device_t)
+    d_oob = torch.zeros(1, dtype=torch.int64, device=device_t)
+    st_ = stream if stream is not None else torch.cuda.current_stream(device_t).cuda_stream
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() else None
+    L = _lib.load()
+    common = (plan.handle, ptr(Yt), ptr(Ro_t), ptr(Gt_t), ptr(Gr_t), float(dt),
+              _lib.DELAY_MULTIPLE if multi else _lib.DELAY_SINGLE, ptr(dl_t), float(cp))
+    if weights is not None:
+        w = torch.as_tensor(weights, dtype=torch.float32, device=device_t).reshape(-1).contiguous()
+        need = Nt if (das_type == _lib.SAFT or Nr == 0) else Nt * Nr
+        if w.numel() != need:
+            raise RuntimeError(f"das: weights need {need} values (one per A-scan column)")
+        _lib.check(L.dream_das_weighted_run_device(*common, ptr(w), ptr(Im), ptr(d_oob),
+                                                   ctypes.c_void_p(st_)))
+    else:
+        _lib.check(L.dream_das_run_device_async(*common, ptr(Im), ptr(d_oob), ctypes.c_void_p(st_)))
+    oob = int(d_oob.item())
+    st = 0 if oob == 0 else {_lib.LVL_IGNORE: 1, _lib.LVL_WARN: 2, _lib.LVL_STOP: 3}[level]
+    _report(st)
+    return Im.cpu().numpy() if on_host else Im

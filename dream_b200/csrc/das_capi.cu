@@ -14,6 +14,7 @@
 #include <string>
 
 #include "../../include/dream_das.h"
+#include "das_fast.h"
 #include "das_kernels.h"
 
 using namespace dream;
@@ -98,7 +99,9 @@ struct dream_das_plan {
   double tri[15] = {0};
   int64_t Nx = 0, Ny = 0, Nz = 0;
   cudaStream_t stream = nullptr;
-  DevBuf bY, bRo, bGt, bGr, bDelay, bIm, bOob;
+  DevBuf bY, bRo, bGt, bGr, bDelay, bIm, bOob, bY16;
+  int64_t n_fast = 0;          // grid hint (0: none)
+  int tile_f = 0, tile_s = 0;  // user / autotuner tile (0: automatic)
   unsigned long long *h_oob = nullptr;  // pinned
   std::atomic<bool> cancelled{false};
   std::atomic<int64_t> launches{0};
@@ -108,6 +111,16 @@ struct dream_das_plan {
 namespace {
 
 size_t prec_size(int prec) { return prec == DREAM_PREC_F64 ? 8 : 4; }
+
+bool is_fast(const dream_das_plan *p) {
+  return p->precision == DREAM_PREC_F32_STORE || p->precision == DREAM_PREC_BF16_STORE;
+}
+// element sizes: Y as passed on the device, geometry, image
+size_t y_dev_size(const dream_das_plan *p) {
+  return p->precision == DREAM_PREC_F64 ? 8 : (p->precision == DREAM_PREC_BF16_STORE ? 2 : 4);
+}
+size_t geo_size(const dream_das_plan *p) { return p->precision == DREAM_PREC_F32 ? 4 : 8; }
+size_t im_size(const dream_das_plan *p) { return p->precision == DREAM_PREC_F64 ? 8 : 4; }
 
 int check_common(int das_type, int64_t K, int64_t No, int64_t Nt, int64_t Nr, int precision) {
   if (das_type < DREAM_DAS_SAFT || das_type > DREAM_DAS_RCA_ROWTX)
@@ -237,11 +250,108 @@ __global__ void add_u64_kernel(unsigned long long *ctr, unsigned long long v) { 
 // K == 0 (or no element pairs) has no in-bounds sample: the image is all
 // zeros and every term is out of bounds.
 int zero_length_ascans(dream_das_plan *p, void *dIm, unsigned long long *doob, cudaStream_t st) {
-  if (p->No > 0) CU(cudaMemsetAsync(dIm, 0, p->No * prec_size(p->precision), st));
+  if (p->No > 0) CU(cudaMemsetAsync(dIm, 0, p->No * im_size(p), st));
   unsigned long long oob = (unsigned long long)p->No * (unsigned long long)terms_per_pixel(p);
   if (doob && oob) {
     add_u64_kernel<<<1, 1, 0, st>>>(doob, oob);
     CU(cudaGetLastError());
+    p->launches++;
+  }
+  return 0;
+}
+
+// Tile of the FP32/BF16-storage kernels: the user's, or the largest CTA
+// whose outer-leg table (n_out x threads x 4 B) fits in 96 KB.
+void fast_tile(const dream_das_plan *p, int n_out, int &tf, int &ts, int &wf) {
+  if (p->tile_f > 0) {
+    tf = p->tile_f;
+    ts = p->tile_s;
+    wf = p->n_fast > 0 ? 8 : 32;
+    return;
+  }
+  int nthr = 256;
+  while (nthr > 32 && (size_t)n_out * nthr * 4 > 96 * 1024) nthr >>= 1;
+  if (p->n_fast > 0) {
+    wf = 8;
+    tf = nthr >= 256 ? 32 : (nthr >= 64 ? 16 : 8);
+    ts = nthr / tf;
+  } else {
+    wf = 32;
+    tf = nthr;
+    ts = 1;
+  }
+}
+
+int launch_fast_plan(dream_das_plan *p, const void *dY, const void *dRo, const void *dGt, const void *dGr,
+                     double dt, int delay_type, const void *ddelay, double cp, const float *dW, float *dIm,
+                     unsigned long long *doob, cudaStream_t st) {
+  if (delay_type != DREAM_DELAY_SINGLE && delay_type != DREAM_DELAY_MULTIPLE)
+    return fail(DREAM_ERR_ARGUMENT, "unknown delay type");
+  if (ddelay == nullptr) return fail(DREAM_ERR_ARGUMENT, "delay pointer is NULL");
+  const int method = effective_method(p);
+  if (method >= DREAM_DAS_RCA_COLTX) {
+    int r = check_rca_edges(p->Nt, p->Nr);
+    if (r) return r;
+  }
+  if (p->No == 0) return 0;
+  if (p->K == 0 || terms_per_pixel(p) == 0) return zero_length_ascans(p, dIm, doob, st);
+  if (dY == nullptr || dRo == nullptr || dGt == nullptr || dIm == nullptr ||
+      (method != DREAM_DAS_SAFT && dGr == nullptr))
+    return fail(DREAM_ERR_ARGUMENT, "NULL device pointer");
+  FastParams F;
+  memset(&F, 0, sizeof(F));
+  F.method = method;
+  F.Y = dY;
+  F.K = p->K;
+  F.Ro = (const double *)dRo;
+  F.No = p->No;
+  F.Gt = (const double *)dGt;
+  F.Nt = (int)p->Nt;
+  F.Gr = (const double *)dGr;
+  F.Nr = (method == DREAM_DAS_SAFT) ? 0 : (int)p->Nr;
+  F.delay = (const double *)ddelay;
+  F.delay_multi = delay_type == DREAM_DELAY_MULTIPLE;
+  Consts64 c = constants_f64(dt, cp, 0.0);
+  F.Fs = c.Fs;
+  F.ocp = c.ocp;
+  F.w = dW;
+  F.Im = dIm;
+  F.oob = doob;
+  const bool bf16 = p->precision == DREAM_PREC_BF16_STORE;
+  const int64_t tpp = std::max<int64_t>(terms_per_pixel(p), 1);
+  if (method == DREAM_DAS_SAFT) {
+    int64_t chunk = std::max<int64_t>(int64_t(1) << 16, (int64_t(1) << 33) / tpp);
+    for (int64_t s0 = 0; s0 < p->No; s0 += chunk) {
+      if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
+      F.no0 = s0;
+      F.no1 = std::min(p->No, s0 + chunk);
+      cudaError_t e = launch_fast(F, bf16, st);
+      if (e != cudaSuccess) return cuda_fail(e, "DAS kernel launch");
+      p->launches++;
+    }
+    return 0;
+  }
+  const int n_out = (method == DREAM_DAS_RCA_ROWTX) ? F.Nr : F.Nt;
+  fast_tile(p, n_out, F.tile_f, F.tile_s, F.wf);
+  if (p->n_fast > 0) {
+    F.n_fast = p->n_fast;
+    F.n_slow = p->No / p->n_fast;
+  } else {
+    F.n_fast = p->No;
+    F.n_slow = 1;
+  }
+  if (fast_smem_bytes(F, F.tile_f * F.tile_s) > 220 * 1024)
+    return fail(DREAM_ERR_UNSUPPORTED, "too many elements on the outer loop for the FP32/BF16 storage kernels");
+  const int64_t slow_tiles = (F.n_slow + F.tile_s - 1) / F.tile_s;
+  const int64_t per_tile_terms = (int64_t)F.tile_s * F.n_fast * tpp;
+  int64_t chunk = std::max<int64_t>(1, (int64_t(1) << 34) / std::max<int64_t>(per_tile_terms, 1));
+  chunk = std::min<int64_t>(chunk, 65535);
+  for (int64_t t0 = 0; t0 < slow_tiles; t0 += chunk) {
+    if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
+    F.slow_tile0 = t0;
+    F.slow_tile1 = std::min(slow_tiles, t0 + chunk);
+    cudaError_t e = launch_fast(F, bf16, st);
+    if (e != cudaSuccess) return cuda_fail(e, "DAS kernel launch");
     p->launches++;
   }
   return 0;
@@ -261,8 +371,6 @@ int dream_das_plan_create(dream_das_plan **plan, int das_type, int64_t a_scan_le
   *plan = nullptr;
   int r = check_common(das_type, a_scan_len, No, num_t_elements, num_r_elements, precision);
   if (r) return r;
-  if (precision != DREAM_PREC_F64 && precision != DREAM_PREC_F32)
-    return fail(DREAM_ERR_UNSUPPORTED, "this plan kind supports F64 and F32 only");
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
@@ -334,9 +442,59 @@ int64_t dream_das_plan_num_ascans(const dream_das_plan *p) { return p ? num_colu
 
 int64_t dream_das_plan_launch_count(const dream_das_plan *p) { return p ? p->launches.load() : -1; }
 
+int dream_das_set_grid_hint(dream_das_plan *p, int64_t n_fast) {
+  if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
+  if (n_fast < 0 || (n_fast > 0 && (p->No % n_fast) != 0))
+    return fail(DREAM_ERR_ARGUMENT, "grid hint must divide the number of image points");
+  std::lock_guard<std::mutex> lk(p->mu);
+  if (n_fast != p->n_fast) p->tile_f = p->tile_s = 0;  // tile shapes depend on the hint
+  p->n_fast = n_fast;
+  return 0;
+}
+
+int dream_das_set_tile(dream_das_plan *p, int tile_f, int tile_s) {
+  if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
+  std::lock_guard<std::mutex> lk(p->mu);
+  if (tile_f == 0 && tile_s == 0) {
+    p->tile_f = p->tile_s = 0;
+    return 0;
+  }
+  const int n = tile_f * tile_s;
+  bool ok = tile_f > 0 && tile_s > 0 && n >= 32 && n <= 256 && n % 32 == 0;
+  if (p->n_fast > 0) ok = ok && tile_f % 8 == 0 && tile_s % 4 == 0;
+  else ok = ok && tile_s == 1;
+  if (!ok) return fail(DREAM_ERR_ARGUMENT, "invalid tile shape");
+  p->tile_f = tile_f;
+  p->tile_s = tile_s;
+  return 0;
+}
+
+int dream_das_get_tile(const dream_das_plan *p, int *tile_f, int *tile_s) {
+  if (p == nullptr || tile_f == nullptr || tile_s == nullptr) return fail(DREAM_ERR_ARGUMENT, "NULL argument");
+  int wf = 0;
+  const int n_out = (effective_method(p) == DREAM_DAS_RCA_ROWTX) ? (int)p->Nr : (int)p->Nt;
+  fast_tile(p, n_out, *tile_f, *tile_s, wf);
+  return 0;
+}
+
+int dream_das_weighted_run_device(dream_das_plan *p, const void *dY, const void *dRo, const void *dGt,
+                                  const void *dGr, double dt, int delay_type, const void *ddelay, double cp,
+                                  const float *dW, float *dIm, unsigned long long *d_oob, void *stream) {
+  if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
+  if (!is_fast(p) || p->uni)
+    return fail(DREAM_ERR_UNSUPPORTED, "weighted DAS needs an F32_STORE or BF16_STORE plan");
+  if (dW == nullptr) return fail(DREAM_ERR_ARGUMENT, "weights pointer is NULL");
+  if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  return launch_fast_plan(p, dY, dRo, dGt, dGr, dt, delay_type, ddelay, cp, dW, dIm, d_oob, (cudaStream_t)stream);
+}
+
 static int run_device_impl(dream_das_plan *p, const void *dY, const void *dRo, const void *dGt, const void *dGr,
                            double dt, int delay_type, const void *ddelay, double cp, void *dIm,
                            unsigned long long *doob, cudaStream_t st) {
+  if (is_fast(p))
+    return launch_fast_plan(p, dY, dRo, dGt, dGr, dt, delay_type, ddelay, cp, nullptr, (float *)dIm, doob, st);
   PlainLaunch L;
   int r = prepare_das(p, L, dY, dRo, dGt, dGr, dt, delay_type, ddelay, cp, dIm, doob);
   if (r) return r;
@@ -386,29 +544,38 @@ int dream_das_run(dream_das_plan *p, const void *Y, const void *Ro, const void *
   std::lock_guard<std::mutex> lk(p->mu);
   DeviceGuard g(p->device);
   cudaStream_t st = p->stream;
-  const size_t es = prec_size(p->precision);
+  const size_t ys = is_fast(p) ? 4 : prec_size(p->precision);  // host Y element
+  const size_t gs = geo_size(p), is = im_size(p);
   const int method = effective_method(p);
   const int64_t ncol = num_columns(p);
   const int64_t nr = (method == DREAM_DAS_SAFT) ? 0 : p->Nr;
   const bool multi = delay_type == DREAM_DELAY_MULTIPLE && p->No != 1;
+  const int64_t ny = p->K * ncol;
   int r;
-  if ((r = p->bY.ensure((size_t)p->K * ncol * es))) return r;
-  if ((r = p->bRo.ensure((size_t)p->No * 3 * es))) return r;
-  if ((r = p->bGt.ensure((size_t)p->Nt * 3 * es))) return r;
-  if ((r = p->bGr.ensure((size_t)nr * 3 * es))) return r;
-  if ((r = p->bDelay.ensure((size_t)(multi ? p->No : 1) * es))) return r;
-  if ((r = p->bIm.ensure((size_t)p->No * es))) return r;
-  if (p->K * ncol > 0) CU(cudaMemcpyAsync(p->bY.p, Y, (size_t)p->K * ncol * es, cudaMemcpyHostToDevice, st));
-  if (p->No > 0) CU(cudaMemcpyAsync(p->bRo.p, Ro, (size_t)p->No * 3 * es, cudaMemcpyHostToDevice, st));
-  if (p->Nt > 0) CU(cudaMemcpyAsync(p->bGt.p, Gt, (size_t)p->Nt * 3 * es, cudaMemcpyHostToDevice, st));
-  if (nr > 0) CU(cudaMemcpyAsync(p->bGr.p, Gr, (size_t)nr * 3 * es, cudaMemcpyHostToDevice, st));
-  CU(cudaMemcpyAsync(p->bDelay.p, delay, (size_t)(multi ? p->No : 1) * es, cudaMemcpyHostToDevice, st));
+  if ((r = p->bY.ensure((size_t)ny * ys))) return r;
+  if ((r = p->bRo.ensure((size_t)p->No * 3 * gs))) return r;
+  if ((r = p->bGt.ensure((size_t)p->Nt * 3 * gs))) return r;
+  if ((r = p->bGr.ensure((size_t)nr * 3 * gs))) return r;
+  if ((r = p->bDelay.ensure((size_t)(multi ? p->No : 1) * gs))) return r;
+  if ((r = p->bIm.ensure((size_t)p->No * is))) return r;
+  if (ny > 0) CU(cudaMemcpyAsync(p->bY.p, Y, (size_t)ny * ys, cudaMemcpyHostToDevice, st));
+  if (p->No > 0) CU(cudaMemcpyAsync(p->bRo.p, Ro, (size_t)p->No * 3 * gs, cudaMemcpyHostToDevice, st));
+  if (p->Nt > 0) CU(cudaMemcpyAsync(p->bGt.p, Gt, (size_t)p->Nt * 3 * gs, cudaMemcpyHostToDevice, st));
+  if (nr > 0) CU(cudaMemcpyAsync(p->bGr.p, Gr, (size_t)nr * 3 * gs, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(p->bDelay.p, delay, (size_t)(multi ? p->No : 1) * gs, cudaMemcpyHostToDevice, st));
+  const void *dYrun = p->bY.p;
+  if (p->precision == DREAM_PREC_BF16_STORE && ny > 0) {
+    if ((r = p->bY16.ensure((size_t)ny * 2))) return r;
+    CU(convert_f32_to_bf16((const float *)p->bY.p, p->bY16.p, ny, st));
+    p->launches++;
+    dYrun = p->bY16.p;
+  }
   unsigned long long *doob = (unsigned long long *)p->bOob.p;
   CU(cudaMemsetAsync(doob, 0, sizeof(unsigned long long), st));
-  r = run_device_impl(p, p->bY.p, p->bRo.p, p->bGt.p, p->bGr.p, dt, delay_type, p->bDelay.p, cp, p->bIm.p,
+  r = run_device_impl(p, dYrun, p->bRo.p, p->bGt.p, p->bGr.p, dt, delay_type, p->bDelay.p, cp, p->bIm.p,
                       doob, st);
   if (r) return r;
-  if (p->No > 0) CU(cudaMemcpyAsync(Im, p->bIm.p, (size_t)p->No * es, cudaMemcpyDeviceToHost, st));
+  if (p->No > 0) CU(cudaMemcpyAsync(Im, p->bIm.p, (size_t)p->No * is, cudaMemcpyDeviceToHost, st));
   CU(cudaMemcpyAsync(p->h_oob, doob, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
   CU(cudaStreamSynchronize(st));
   uint64_t oob = *p->h_oob;

@@ -1,0 +1,36 @@
+// das_fast.h -- launch descriptor of the FP32/BF16-storage DAS kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dream {
+
+struct FastParams {
+  int method;  // 0 SAFT, 1 TFM, 2 RCA col-tx, 3 RCA row-tx
+  const void *Y;  // float or bf16, K x (Nt*Nr) column-major
+  int64_t K;
+  const double *Ro;
+  int64_t No;
+  const double *Gt;
+  int Nt;
+  const double *Gr;
+  int Nr;
+  const double *delay;  // us; 1 value or No values
+  int delay_multi;
+  double Fs, ocp;  // (1/dt)*1000 and 1/cp in FP64, as DAS<double>
+  const float *w;  // per A-scan column weights, or nullptr
+  float *Im;
+  unsigned long long *oob;
+  // image tiling: point n = s*n_fast + f
+  int64_t n_fast, n_slow;
+  int tile_f, tile_s, wf;  // tile extents; warp lanes along the fast axis
+  int64_t slow_tile0, slow_tile1;  // slow-tile range of this launch
+  int64_t no0, no1;                // point range (SAFT launches)
+};
+
+size_t fast_smem_bytes(const FastParams &P, int nthr);
+cudaError_t launch_fast(const FastParams &P, bool bf16, cudaStream_t st);
+cudaError_t convert_f32_to_bf16(const float *x, void *y, int64_t n, cudaStream_t st);
+
+}  // namespace dream

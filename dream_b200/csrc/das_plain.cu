@@ -45,15 +45,12 @@ struct PlainParams {
   int64_t Nx, Ny, Nz;
 };
 
-template <class T>
-__device__ __forceinline__ int to_index(T p, int bigk);
-template <>
-__device__ __forceinline__ int to_index<double>(double p, int) {
+// Truncation of p in (-1, K). Long A-scans (FP32, K >= 2^22) need the
+// conversion unit; every other case uses the exact add-based form.
+template <class T, bool BIGK>
+__device__ __forceinline__ int to_index(T p) {
+  if (BIGK) return __float2int_rz((float)p);
   return trunc_index(p);
-}
-template <>
-__device__ __forceinline__ int to_index<float>(float p, int bigk) {
-  return bigk ? __float2int_rz(p) : trunc_index(p);
 }
 
 // delay / 1000 the way each reference form computes it: DAS<double> in
@@ -63,7 +60,9 @@ __device__ __forceinline__ float delay_to_ms(float d) {
   return __double2float_rn((double)d / 1000.0);
 }
 
-template <class T, int M, bool UNI, bool TAB>
+constexpr int UNROLL = 8;  // gathers in flight per thread before their in-order adds
+
+template <class T, int M, bool UNI, bool TAB, bool BIGK>
 __global__ void __launch_bounds__(256) das_plain_kernel(const PlainParams<T> P) {
   using A = Ar<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -178,7 +177,7 @@ __global__ void __launch_bounds__(256) das_plain_kernel(const PlainParams<T> P) 
       T tdp = A::mul((T)2, t);  // exact doubling, as 2.0*t_tr
       T p = A::mul(tdp, P.Fs);
       if (p > (T)-1 && p < P.Kf) {
-        im = A::add(im, __ldg(ycol + to_index(p, P.bigk)));
+        im = A::add(im, __ldg(ycol + to_index<T, BIGK>(p)));
       } else {
         oob++;
       }
@@ -207,11 +206,31 @@ __global__ void __launch_bounds__(256) das_plain_kernel(const PlainParams<T> P) 
       else if (M == RCA_COLTX) lo = leg_col(o);
       else lo = leg_row(o);
       if (delay_outer) lo = A::add(lo, delay_ms);
-      for (int i = 0; i < n_in; i++) {
+      int i = 0;
+      // UNROLL terms at a time: all gathers are issued before the adds, which
+      // then run in the reference order (the sum is unchanged bit for bit).
+      for (; i + UNROLL <= n_in; i += UNROLL) {
+        T y[UNROLL];
+        bool v[UNROLL];
+#pragma unroll
+        for (int u = 0; u < UNROLL; u++) {
+          T li = TAB ? tab[(i + u) * bd + tid] : inner_leg(i + u);
+          T p = A::mul(A::add(lo, li), P.Fs);
+          v[u] = p > (T)-1 && p < P.Kf;
+          y[u] = v[u] ? __ldg(ycol + (int64_t)u * P.K + to_index<T, BIGK>(p)) : (T)0;
+        }
+#pragma unroll
+        for (int u = 0; u < UNROLL; u++) {
+          if (v[u]) im = A::add(im, y[u]);
+          else oob++;
+        }
+        ycol += UNROLL * P.K;
+      }
+      for (; i < n_in; i++) {
         T li = TAB ? tab[i * bd + tid] : inner_leg(i);
         T p = A::mul(A::add(lo, li), P.Fs);
         if (p > (T)-1 && p < P.Kf) {
-          im = A::add(im, __ldg(ycol + to_index(p, P.bigk)));
+          im = A::add(im, __ldg(ycol + to_index<T, BIGK>(p)));
         } else {
           oob++;
         }
@@ -229,7 +248,8 @@ __global__ void __launch_bounds__(256) das_plain_kernel(const PlainParams<T> P) 
 
 template <class T, int M, bool UNI, bool TAB>
 static cudaError_t launch_one(const PlainParams<T> &P, int bd, size_t smem, cudaStream_t st) {
-  auto kern = das_plain_kernel<T, M, UNI, TAB>;
+  auto kern = (sizeof(T) == 4 && P.bigk) ? das_plain_kernel<T, M, UNI, TAB, true>
+                                         : das_plain_kernel<T, M, UNI, TAB, false>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

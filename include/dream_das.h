@@ -170,6 +170,39 @@ int dream_das_uni_run_device(dream_das_plan *plan, const void *dY, const double 
 /* Number of kernels this plan has launched since it was created. */
 int64_t dream_das_plan_launch_count(const dream_das_plan *plan);
 
+/*
+ * Image-grid hint for the F32_STORE / BF16_STORE kernels: image point n is
+ * (n mod n_fast, n / n_fast) on a regular 2-D (or flattened 3-D) grid whose
+ * fastest axis has n_fast points, e.g. Nz for Ro = meshgrid(x, z) flattened
+ * column-major. Points adjacent on both axes are then processed by the same
+ * CTA. 0 removes the hint (consecutive points are grouped). Any value gives
+ * the same image; only speed depends on it. No must be a multiple of n_fast.
+ */
+int dream_das_set_grid_hint(dream_das_plan *plan, int64_t n_fast);
+
+/*
+ * Tile of image points per CTA for the F32_STORE / BF16_STORE kernels:
+ * tile_f points along the fast grid axis x tile_s along the slow axis
+ * (tile_f*tile_s threads, 32..256, a multiple of 32; with a grid hint tile_f
+ * is a multiple of 8 and tile_s of 4, without one tile_s must be 1).
+ * (0, 0) restores the automatic choice. Used by the autotuner.
+ */
+int dream_das_set_tile(dream_das_plan *plan, int tile_f, int tile_s);
+int dream_das_get_tile(const dream_das_plan *plan, int *tile_f, int *tile_s);
+
+/*
+ * Weighted DAS, the forward operator of the differentiable beamformer:
+ *   Im[n] = sum over A-scan columns c of w[c] * Y[k(n, c), c]
+ * with k the FP64-exact sample index of the plain method. F32_STORE and
+ * BF16_STORE plans only; dW holds one float per A-scan column (Nt for SAFT,
+ * Nt*Nr otherwise, in Y's column order). Asynchronous like
+ * dream_das_run_device_async.
+ */
+int dream_das_weighted_run_device(dream_das_plan *plan, const void *dY, const void *dRo,
+                                  const void *dGt, const void *dGr, double dt, int delay_type,
+                                  const void *ddelay, double cp, const float *dW, float *dIm,
+                                  unsigned long long *d_oob, void *stream);
+
 /* Requests cancellation: running and later calls return DREAM_ERR_CANCELLED
  * between launches until dream_das_set_running is called. */
 void dream_das_cancel(dream_das_plan *plan);

@@ -1,0 +1,205 @@
+"""FP32/BF16-storage DAS (precision upgrade) against the FP64 oracle.
+
+Index exactness is checked two ways:
+  * index reveal: one element pair and Y[:,0] = k+1 stored exactly in FP32, so
+    the image is the selected FP64 index + 1 for every pixel;
+  * white-noise A-scans: the oracle sums exactly the same stored (rounded)
+    samples in FP64; any wrong index moves a pixel by O(1) while the FP32
+    compensated sum stays within 1e-6 of max|Im|.
+Image error against the FP64 oracle on the original FP64 A-scans is bounded
+by 1e-5 (FP32 storage) and 1e-3 (BF16 storage) relative to max|Im|.
+"""
+import numpy as np
+import pytest
+
+from cases import CASES, _index_reveal, _near_element, build_scene
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def bf16_round(a):
+    t = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(torch.bfloat16).to(torch.float64)
+    return np.asfortranarray(t.numpy())
+
+
+def mixed(s, storage="f32", **kw):
+    from dream_b200.beamformer import das_mixed
+    Gr = s.Gr if s.method != "saft" else None
+    return das_mixed(s.Y, s.Gt, Gr, s.Ro, s.dt, s.delay, s.cp, s.method, kw.pop("err", "ignore"), "cuda",
+                     storage, **kw)
+
+
+def oracle_on_stored(s, storage, err="ignore"):
+    Ys = np.asfortranarray(s.Y.astype(np.float32).astype(np.float64)) if storage == "f32" else bf16_round(s.Y)
+    return oracle.das(Ys, s.Gt, s.Gr, s.Ro, s.dt, s.delay, s.cp, s.method, err, np.float64)
+
+
+@pytest.mark.parametrize("hint", ["auto", 0])
+@pytest.mark.parametrize("grid", [(512, 512, (-20.0, 20.0), (2.0, 50.0)), (96, 96, (-20.0, 20.0), (0.0, 50.0))])
+def test_index_reveal_fp64_indices(hint, grid):
+    nx, nz, xr, zr = grid
+    s = _index_reveal(K=3000, nx=nx, nz=nz, x_rng=xr, z_rng=zr)
+    _, _, _, idx = oracle.das(s.Y, s.Gt, s.Gr, s.Ro, s.dt, s.delay, s.cp, "tfm", "ignore", np.float64,
+                              return_idx=True)
+    Im = mixed(s, hint=hint)
+    k = np.where(idx[0] == oracle.OOB_MISS, -1, idx[0])
+    assert np.array_equal(Im.astype(np.int64) - 1, k)
+
+
+@pytest.mark.parametrize("delay", [-0.03, -0.045, 0.0])
+def test_near_element_truncation(delay):
+    s = _near_element(delay)
+    ref, st, oob = oracle.das(s.Y, s.Gt, s.Gr, s.Ro, s.dt, s.delay, s.cp, "tfm", "ignore", np.float64)
+    Im = mixed(s)
+    assert np.array_equal(Im.astype(np.float64), ref)
+
+
+def test_lattice_exact_integer_times():
+    """Distances of 3-4-5 triangles at cp = 1000 m/s and dt = 1 us put many
+    products t*Fs on (or within rounding of) integers: the ambiguous-band
+    path must reproduce the FP64 truncation."""
+    from dream_b200 import synth
+    G = np.asfortranarray(np.array([[0.0, 0.0, 0.0], [3.0, 0.0, 0.0], [-4.0, 0.0, 0.0], [6.0, 0.0, 0.0]]))
+    xs = np.arange(-12.0, 12.5, 1.0)
+    zs = np.arange(0.0, 16.5, 1.0)
+    X, Z = np.meshgrid(xs, zs)
+    Ro = np.asfortranarray(np.stack([X.flatten("F"), np.zeros(X.size), Z.flatten("F")], 1))
+    K = 64
+    rng = np.random.default_rng(3)
+    Y = np.asfortranarray(rng.normal(size=(K, 16)))
+    s = synth.Scene(Y, G, G.copy(order="F"), Ro, 1.0, np.zeros((1, 1)), 1000.0, "tfm", (xs.size, zs.size))
+    ref, st, oob = oracle_on_stored(s, "f32")
+    Im = mixed(s)
+    assert np.abs(Im - ref).max() <= 1e-6 * np.abs(ref).max()
+    _, _, oob_g = oracle.das(s.Y, s.Gt, s.Gr, s.Ro, s.dt, s.delay, s.cp, "tfm", "ignore", np.float64)
+    assert oob == oob_g
+
+
+NOISE_CASES = [
+    ("tfm", dict(kind="tfm", kw=dict(seed=31, n_el=16, K=3000, nx=40, nz=48))),
+    ("tfm_delay", dict(kind="tfm", kw=dict(seed=32, n_el=12, K=3000, nx=33, nz=40), delay=0.41)),
+    ("tfm_delayvec", dict(kind="tfm", kw=dict(seed=13, n_el=8, K=3000, nx=16, nz=40), delay_vector_seed=5)),
+    ("tfm_oob", dict(kind="tfm", kw=dict(seed=16, n_el=8, K=700, nx=16, nz=16))),
+    ("saft", dict(kind="saft", kw=dict(seed=33, n_el=32, K=2048, nx=48, nz=40))),
+    ("saft_oob", dict(kind="saft", kw=dict(seed=17, n_el=8, K=400, nx=16, nz=16))),
+    ("rca_coltx", dict(kind="rca", kw=dict(seed=34, n_cols=16, n_rows=16, K=4096, nx=8, ny=8, nz=16,
+                                           method="rca_coltx"), delay=0.11)),
+    ("rca_rowtx", dict(kind="rca", kw=dict(seed=35, n_cols=16, n_rows=16, K=4096, nx=8, ny=8, nz=16,
+                                           method="rca_rowtx"), delay=0.11)),
+    ("rca_mixed", dict(kind="rca", kw=dict(seed=15, n_cols=8, n_rows=10, K=4096, nx=5, ny=7, nz=6,
+                                           method="rca_rowtx"))),
+]
+
+
+@pytest.mark.parametrize("storage", ["f32", "bf16"])
+@pytest.mark.parametrize("name,spec", NOISE_CASES, ids=[c[0] for c in NOISE_CASES])
+def test_noise_ascans_exact_indices(name, spec, storage):
+    s = build_scene(spec)
+    rng = np.random.default_rng(99)
+    s.Y = np.asfortranarray(rng.normal(size=s.Y.shape))
+    ref, st, oob = oracle_on_stored(s, storage)
+    Im = mixed(s, storage)
+    scale = max(np.abs(ref).max(), 1e-30)
+    assert np.abs(Im - ref).max() <= 1e-6 * scale, f"max rel err {np.abs(Im - ref).max() / scale:.3e}"
+
+
+# FP32 storage: within 1e-5 of max|Im|. BF16 keeps 8 significant bits, so a
+# stored sample is off by at most 2^-9 of its magnitude; the per-pixel error is
+# bounded by 2^-9 * sum|y| over the selected samples (checked with a factor 2
+# for the FP32 sums). Small element counts (the 16-element SAFT, 12x12 RCA
+# cases here) keep most of that; the full configurations meet 1e-3 of max|Im|
+# (test_tfm_full_config, test_rca_full_config_bf16).
+@pytest.mark.parametrize("storage", ["f32", "bf16"])
+@pytest.mark.parametrize("name", ["tfm_f64", "saft_f64", "rca_coltx_f64", "rca_rowtx_f64", "tfm_delayvec_f64"])
+def test_image_error_vs_fp64_oracle(name, storage):
+    s = build_scene(CASES[name])
+    ref, _, _ = oracle.das(s.Y, s.Gt, s.Gr, s.Ro, s.dt, s.delay, s.cp, s.method, "ignore", np.float64)
+    Im = mixed(s, storage)
+    if storage == "f32":
+        assert np.abs(Im - ref).max() <= 1e-5 * np.abs(ref).max()
+    else:
+        absum, _, _ = oracle.das(np.abs(s.Y), s.Gt, s.Gr, s.Ro, s.dt, s.delay, s.cp, s.method, "ignore")
+        assert np.all(np.abs(Im - ref) <= 2.0 ** -8 * absum + 1e-6 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("tile", [(8, 4), (16, 8), (32, 8), (8, 32), (32, 4), (64, 4)])
+def test_tile_shapes_same_image(tile):
+    s = build_scene(dict(kind="tfm", kw=dict(seed=36, n_el=16, K=3000, nx=40, nz=48)))
+    rng = np.random.default_rng(5)
+    s.Y = np.asfortranarray(rng.normal(size=s.Y.shape))
+    ref, _, _ = oracle_on_stored(s, "f32")
+    Im = mixed(s, tile=tile)
+    assert np.abs(Im - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
+def test_unhinted_tiles():
+    s = build_scene(dict(kind="tfm", kw=dict(seed=37, n_el=16, K=3000, nx=24, nz=50)))
+    rng = np.random.default_rng(6)
+    s.Y = np.asfortranarray(rng.normal(size=s.Y.shape))
+    ref, _, _ = oracle_on_stored(s, "f32")
+    for tile in [None, (64, 1), (32, 1)]:
+        Im = mixed(s, hint=0, tile=tile)
+        assert np.abs(Im - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
+def test_oob_levels_and_counts(capsys):
+    s = build_scene(dict(kind="tfm", kw=dict(seed=16, n_el=8, K=700, nx=16, nz=16)))
+    with pytest.raises(RuntimeError, match="out-of-bounds"):
+        mixed(s, err="stop")
+    mixed(s, err="warn")
+    assert "Warning: DAS out-of-bounds!" in capsys.readouterr().out
+
+
+def test_weighted_matches_oracle():
+    s = build_scene(dict(kind="tfm", kw=dict(seed=38, n_el=8, K=1500, nx=20, nz=30)))
+    rng = np.random.default_rng(7)
+    s.Y = np.asfortranarray(rng.normal(size=s.Y.shape))
+    _, _, _, idx = oracle.das(s.Y, s.Gt, s.Gr, s.Ro, s.dt, s.delay, s.cp, "tfm", "ignore", np.float64,
+                              return_idx=True)
+    w = rng.uniform(0.2, 1.5, idx.shape[0])
+    Ys = s.Y.astype(np.float32).astype(np.float64)
+    ref = oracle.weighted(idx, Ys, w.astype(np.float32).astype(np.float64))
+    Im = mixed(s, weights=w)
+    assert np.abs(Im - ref).max() <= 2e-6 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("storage,tol", [("f32", 1e-5), ("bf16", 1e-3)])
+def test_tfm_full_config(storage, tol):
+    """The TFM configuration (64x64 FMC, K=3000, 512x512): image error vs the
+    FP64 reference on 4096 seeded pixels."""
+    from dream_b200 import synth
+    s = synth.tfm_scene(seed=1)
+    Im = mixed(s, storage)
+    sel = np.sort(np.random.default_rng(7).choice(s.Ro.shape[0], 4096, replace=False))
+    sub = s.astype(np.float64)
+    sub.Ro = np.asfortranarray(s.Ro[sel])
+    mod = oracle.reference_module("f64")
+    if mod is not None:
+        ref = mod.das(sub.Y, sub.Gt, sub.Gr, sub.Ro, sub.dt, sub.delay, sub.cp, "tfm", "stop", "cpu", "")
+    else:
+        ref = oracle.das(sub.Y, sub.Gt, sub.Gr, sub.Ro, sub.dt, sub.delay, sub.cp, "tfm", "stop")[0]
+    full_ref_scale = np.abs(ref).max()
+    assert np.abs(Im[sel] - ref).max() <= tol * full_ref_scale
+
+
+def test_rca_full_config_bf16():
+    """RCA configuration (128x128 RCA, K=4096, 128x128x256 grid), BF16 storage:
+    1024 seeded pixels vs the FP64 oracle within 1e-3 of max|Im| (taken over
+    the checked pixels and the GPU image)."""
+    from dream_b200 import synth
+    s = synth.rca_scene(seed=2)
+    Im = mixed(s, "bf16")
+    sel = np.sort(np.random.default_rng(8).choice(s.Ro.shape[0], 1024, replace=False))
+    sub = s.astype(np.float64)
+    sub.Ro = np.asfortranarray(s.Ro[sel])
+    ref = oracle.das(sub.Y, sub.Gt, sub.Gr, sub.Ro, sub.dt, sub.delay, sub.cp, s.method, "ignore")[0]
+    scale = max(np.abs(Im).max(), np.abs(ref).max())
+    assert np.abs(Im[sel] - ref).max() <= 1e-3 * scale
