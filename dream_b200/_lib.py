@@ -51,8 +51,14 @@ SIGNATURES = {
     "dream_das_uni_run_device": (_i, [_vp, _vp, _pd, _d, _d, _d, _vp, _i, _pi64, _vp]),
     "dream_das_set_grid_hint": (_i, [_vp, _i64]),
     "dream_das_set_tile": (_i, [_vp, _i, _i]),
+    "dream_das_set_chunk": (_i, [_vp, _i]),
     "dream_das_get_tile": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "dream_das_weighted_run_device": (_i, [_vp, _vp, _vp, _vp, _vp, _d, _i, _vp, _d, _vp, _vp, _vp, _vp]),
+    "dream_das_bind_geometry": (_i, [_vp, _vp, _vp, _vp, _d, _i, _vp, _d, _vp]),
+    "dream_das_op_forward": (_i, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "dream_das_op_adjoint": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "dream_das_op_wgrad": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "dream_das_op_backward": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dream_das_cancel": (None, [_vp]),
     "dream_das_set_running": (None, [_vp]),
 }

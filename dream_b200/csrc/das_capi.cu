@@ -102,6 +102,12 @@ struct dream_das_plan {
   DevBuf bY, bRo, bGt, bGr, bDelay, bIm, bOob, bY16;
   int64_t n_fast = 0;          // grid hint (0: none)
   int tile_f = 0, tile_s = 0;  // user / autotuner tile (0: automatic)
+  int jc = 0;                  // user / autotuner inner chunk (0: automatic)
+  // geometry-bound operator
+  bool bound = false;
+  FastParams geo{};
+  DevBuf bTA, bTB, bRange;
+  int sm_count = 148;
   unsigned long long *h_oob = nullptr;  // pinned
   std::atomic<bool> cancelled{false};
   std::atomic<int64_t> launches{0};
@@ -333,6 +339,7 @@ int launch_fast_plan(dream_das_plan *p, const void *dY, const void *dRo, const v
   }
   const int n_out = (method == DREAM_DAS_RCA_ROWTX) ? F.Nr : F.Nt;
   fast_tile(p, n_out, F.tile_f, F.tile_s, F.wf);
+  F.jc = p->jc ? p->jc : 16;
   if (p->n_fast > 0) {
     F.n_fast = p->n_fast;
     F.n_slow = p->No / p->n_fast;
@@ -396,6 +403,7 @@ int dream_das_plan_create(dream_das_plan **plan, int das_type, int64_t a_scan_le
     dream_das_plan_destroy(p);
     return r;
   }
+  cudaDeviceGetAttribute(&p->sm_count, cudaDevAttrMultiProcessorCount, device);
   *plan = p;
   return 0;
 }
@@ -422,6 +430,10 @@ void dream_das_plan_destroy(dream_das_plan *p) {
     p->bDelay.release();
     p->bIm.release();
     p->bOob.release();
+    p->bY16.release();
+    p->bTA.release();
+    p->bTB.release();
+    p->bRange.release();
     if (p->h_oob) cudaFreeHost(p->h_oob);
     if (p->stream) cudaStreamDestroy(p->stream);
   }
@@ -469,12 +481,138 @@ int dream_das_set_tile(dream_das_plan *p, int tile_f, int tile_s) {
   return 0;
 }
 
+int dream_das_set_chunk(dream_das_plan *p, int jc) {
+  if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
+  if (jc != 0 && jc != 8 && jc != 16) return fail(DREAM_ERR_ARGUMENT, "chunk must be 0, 8 or 16");
+  std::lock_guard<std::mutex> lk(p->mu);
+  p->jc = jc;
+  return 0;
+}
+
 int dream_das_get_tile(const dream_das_plan *p, int *tile_f, int *tile_s) {
   if (p == nullptr || tile_f == nullptr || tile_s == nullptr) return fail(DREAM_ERR_ARGUMENT, "NULL argument");
   int wf = 0;
   const int n_out = (effective_method(p) == DREAM_DAS_RCA_ROWTX) ? (int)p->Nr : (int)p->Nt;
   fast_tile(p, n_out, *tile_f, *tile_s, wf);
   return 0;
+}
+
+int dream_das_bind_geometry(dream_das_plan *p, const void *dRo, const void *dGt, const void *dGr, double dt,
+                            int delay_type, const void *ddelay, double cp, void *stream) {
+  if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
+  if (p->precision != DREAM_PREC_F32_STORE || p->uni)
+    return fail(DREAM_ERR_UNSUPPORTED, "the differentiable operator needs an F32_STORE plan");
+  if (delay_type != DREAM_DELAY_SINGLE && delay_type != DREAM_DELAY_MULTIPLE)
+    return fail(DREAM_ERR_ARGUMENT, "unknown delay type");
+  const int method = effective_method(p);
+  if (method == DREAM_DAS_SAFT) return fail(DREAM_ERR_UNSUPPORTED, "the operator supports TFM and RCA");
+  if (method >= DREAM_DAS_RCA_COLTX) {
+    int r = check_rca_edges(p->Nt, p->Nr);
+    if (r) return r;
+  }
+  if ((p->No > 0 && dRo == nullptr) || dGt == nullptr || dGr == nullptr || ddelay == nullptr)
+    return fail(DREAM_ERR_ARGUMENT, "NULL device pointer");
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  FastParams F;
+  memset(&F, 0, sizeof(F));
+  F.method = method;
+  F.K = p->K;
+  F.Ro = (const double *)dRo;
+  F.No = p->No;
+  F.Gt = (const double *)dGt;
+  F.Nt = (int)p->Nt;
+  F.Gr = (const double *)dGr;
+  F.Nr = (int)p->Nr;
+  F.delay = (const double *)ddelay;
+  F.delay_multi = delay_type == DREAM_DELAY_MULTIPLE;
+  Consts64 c = constants_f64(dt, cp, 0.0);
+  F.Fs = c.Fs;
+  F.ocp = c.ocp;
+  int r;
+  const int n_out = (method == DREAM_DAS_RCA_ROWTX) ? F.Nr : F.Nt;
+  const int n_in = (method == DREAM_DAS_RCA_ROWTX) ? F.Nt : F.Nr;
+  if ((r = p->bTA.ensure((size_t)n_out * p->No * 8))) return r;
+  if ((r = p->bTB.ensure((size_t)n_in * p->No * 8))) return r;
+  if ((r = p->bRange.ensure(8 * sizeof(int)))) return r;
+  CU(build_leg_tables(F, (int64_t *)p->bTA.p, (int64_t *)p->bTB.p, (int *)p->bRange.p, st));
+  p->launches += 2;
+  p->geo = F;
+  p->bound = true;
+  return 0;
+}
+
+static int op_check(dream_das_plan *p) {
+  if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
+  if (!p->bound) return fail(DREAM_ERR_ARGUMENT, "no geometry bound (dream_das_bind_geometry)");
+  if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
+  return 0;
+}
+
+int dream_das_op_forward(dream_das_plan *p, const float *dY, const float *dW, float *dIm, unsigned long long *d_oob,
+                         void *stream) {
+  int r = op_check(p);
+  if (r) return r;
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  if (p->No == 0) return 0;
+  if (p->K == 0) return zero_length_ascans(p, dIm, d_oob, (cudaStream_t)stream);
+  FastParams F = p->geo;
+  F.Y = dY;
+  F.w = dW;
+  F.Im = dIm;
+  F.oob = d_oob;
+  CU(launch_tab_gather(F, (const int64_t *)p->bTA.p, (const int64_t *)p->bTB.p, (const int *)p->bRange.p,
+                       (cudaStream_t)stream));
+  p->launches++;
+  return 0;
+}
+
+static int op_colowner(dream_das_plan *p, const float *X, const float *G, const float *dY, const float *dW, float *Ya,
+                       float *dWg, bool adj, bool wg, cudaStream_t st) {
+  const size_t ycount = (size_t)p->K * num_columns(p);
+  if (adj && ycount) CU(cudaMemsetAsync(Ya, 0, ycount * 4, st));
+  if (wg) CU(cudaMemsetAsync(dWg, 0, (size_t)num_columns(p) * 4, st));
+  if (p->No == 0 || p->K == 0) return 0;
+  FastParams F = p->geo;
+  F.Y = dY;
+  F.w = dW;
+  cudaError_t e = launch_tab_colowner(F, (const int64_t *)p->bTA.p, (const int64_t *)p->bTB.p, X, G, Ya, dWg, adj,
+                                      wg, p->sm_count, st);
+  if (e == cudaErrorInvalidValue) return fail(DREAM_ERR_UNSUPPORTED, "A-scans too long for the adjoint histogram");
+  if (e != cudaSuccess) return cuda_fail(e, "adjoint kernel launch");
+  p->launches++;
+  return 0;
+}
+
+int dream_das_op_adjoint(dream_das_plan *p, const float *dX, const float *dW, float *dYa, void *stream) {
+  int r = op_check(p);
+  if (r) return r;
+  if (dX == nullptr || dYa == nullptr) return fail(DREAM_ERR_ARGUMENT, "NULL device pointer");
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  return op_colowner(p, dX, nullptr, nullptr, dW, dYa, nullptr, true, false, (cudaStream_t)stream);
+}
+
+int dream_das_op_wgrad(dream_das_plan *p, const float *dG, const float *dY, float *dWgrad, void *stream) {
+  int r = op_check(p);
+  if (r) return r;
+  if (dG == nullptr || dY == nullptr || dWgrad == nullptr) return fail(DREAM_ERR_ARGUMENT, "NULL device pointer");
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  return op_colowner(p, nullptr, dG, dY, nullptr, nullptr, dWgrad, false, true, (cudaStream_t)stream);
+}
+
+int dream_das_op_backward(dream_das_plan *p, const float *dG, const float *dY, const float *dW, float *dYgrad,
+                          float *dWgrad, void *stream) {
+  int r = op_check(p);
+  if (r) return r;
+  if (dG == nullptr || dYgrad == nullptr || dWgrad == nullptr || dY == nullptr)
+    return fail(DREAM_ERR_ARGUMENT, "NULL device pointer");
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  return op_colowner(p, dG, dG, dY, dW, dYgrad, dWgrad, true, true, (cudaStream_t)stream);
 }
 
 int dream_das_weighted_run_device(dream_das_plan *p, const void *dY, const void *dRo, const void *dGt,

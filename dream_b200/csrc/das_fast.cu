@@ -37,7 +37,6 @@ namespace {
 constexpr int FB = 24;                 // fraction bits of the relative legs
 constexpr uint32_t DELTA_UNITS = 4;    // delta = 2^-22 in 2^-24 units
 constexpr uint32_t AMB_LO = 8u << 8;   // 2*delta in the 2^-32 units of the low word
-constexpr int JC = 16;                 // inner elements per register chunk
 constexpr int MAX_EXTENT = 126;        // max integer spread of a leg over a tile
 
 template <class YT>
@@ -180,7 +179,7 @@ __device__ __noinline__ float exact_partial(const FastParams &P, const Pixel &px
 // issued unconditionally: in an in-bounds tile every floor index, ambiguous
 // or not, lies inside its A-scan. Ambiguity is tracked as the minimum
 // fraction word; a chunk whose minimum falls in the band is recomputed.
-template <class YT, bool WEIGHTED, bool CHECKED, bool FULL>
+template <class YT, bool WEIGHTED, bool CHECKED, bool FULL, int JC>
 __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &px, const uint64_t (&B64)[JC],
                                              uint64_t A64, int64_t colbase, int o, int i0, int jn, int n_in,
                                              unsigned int &oob) {
@@ -233,7 +232,7 @@ __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &p
   return part;
 }
 
-template <class YT, bool WEIGHTED, bool CHECKED>
+template <class YT, bool WEIGHTED, bool CHECKED, int JC>
 __device__ __forceinline__ void tile_loop(const FastParams &P, const Pixel &px, const TileShared &S, int tid,
                                           int nthr, int n_out, int n_in, float &acc_s, float &acc_c,
                                           unsigned int &oob) {
@@ -260,21 +259,21 @@ __device__ __forceinline__ void tile_loop(const FastParams &P, const Pixel &px, 
       for (; o + 2 <= n_out; o += 2) {
         const uint64_t A0 = ((uint64_t)S.arel[o * nthr + tid] << 8) + ((uint64_t)S.ahi[o] << 32);
         const uint64_t A1 = ((uint64_t)S.arel[(o + 1) * nthr + tid] << 8) + ((uint64_t)S.ahi[o + 1] << 32);
-        float part = chunk_terms<YT, WEIGHTED, CHECKED, true>(P, px, B64, A0, (int64_t)o * n_in, o, i0, JC,
+        float part = chunk_terms<YT, WEIGHTED, CHECKED, true, JC>(P, px, B64, A0, (int64_t)o * n_in, o, i0, JC,
                                                              n_in, oob);
-        part += chunk_terms<YT, WEIGHTED, CHECKED, true>(P, px, B64, A1, (int64_t)(o + 1) * n_in, o + 1, i0,
+        part += chunk_terms<YT, WEIGHTED, CHECKED, true, JC>(P, px, B64, A1, (int64_t)(o + 1) * n_in, o + 1, i0,
                                                         JC, n_in, oob);
         neumaier(acc_s, acc_c, part);
       }
       for (; o < n_out; o++) {
         const uint64_t A0 = ((uint64_t)S.arel[o * nthr + tid] << 8) + ((uint64_t)S.ahi[o] << 32);
         neumaier(acc_s, acc_c,
-                 chunk_terms<YT, WEIGHTED, CHECKED, true>(P, px, B64, A0, (int64_t)o * n_in, o, i0, JC, n_in, oob));
+                 chunk_terms<YT, WEIGHTED, CHECKED, true, JC>(P, px, B64, A0, (int64_t)o * n_in, o, i0, JC, n_in, oob));
       }
     } else {
       for (int o = 0; o < n_out; o++) {
         const uint64_t A64 = ((uint64_t)S.arel[o * nthr + tid] << 8) + ((uint64_t)S.ahi[o] << 32);
-        neumaier(acc_s, acc_c, chunk_terms<YT, WEIGHTED, CHECKED, false>(P, px, B64, A64, (int64_t)o * n_in, o,
+        neumaier(acc_s, acc_c, chunk_terms<YT, WEIGHTED, CHECKED, false, JC>(P, px, B64, A64, (int64_t)o * n_in, o,
                                                                          i0, jn, n_in, oob));
       }
     }
@@ -283,7 +282,7 @@ __device__ __forceinline__ void tile_loop(const FastParams &P, const Pixel &px, 
 
 }  // namespace
 
-template <class YT, bool WEIGHTED>
+template <class YT, bool WEIGHTED, int JC>
 __global__ void __launch_bounds__(256) das_fast_kernel(const FastParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int tid = threadIdx.x;
@@ -396,8 +395,8 @@ __global__ void __launch_bounds__(256) das_fast_kernel(const FastParams P) {
       S.arel[o * nthr + tid] = S.arel[o * nthr + tid] - ((uint32_t)S.minA[o] << FB) + DELTA_UNITS;
     for (int o = tid; o < n_out; o += nthr) S.ahi[o] = (uint32_t)((int64_t)o * n_in * P.K + S.minA[o]);
     __syncthreads();
-    if (in_bounds) tile_loop<YT, WEIGHTED, false>(P, px, S, tid, nthr, n_out, n_in, acc_s, acc_c, oob);
-    else tile_loop<YT, WEIGHTED, true>(P, px, S, tid, nthr, n_out, n_in, acc_s, acc_c, oob);
+    if (in_bounds) tile_loop<YT, WEIGHTED, false, JC>(P, px, S, tid, nthr, n_out, n_in, acc_s, acc_c, oob);
+    else tile_loop<YT, WEIGHTED, true, JC>(P, px, S, tid, nthr, n_out, n_in, acc_s, acc_c, oob);
   }
   if (active) P.Im[no] = acc_s + acc_c;
   add_count(P.oob, active ? oob : 0u);
@@ -461,7 +460,7 @@ static cudaError_t launch_fast_t(const FastParams &P, cudaStream_t st) {
   }
   const int nthr = P.tile_f * P.tile_s;
   const size_t smem = fast_smem_bytes(P, nthr);
-  auto kern = das_fast_kernel<YT, W>;
+  auto kern = (P.jc == 8) ? das_fast_kernel<YT, W, 8> : das_fast_kernel<YT, W, 16>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const int64_t gx = (P.n_fast + P.tile_f - 1) / P.tile_f;
@@ -482,6 +481,267 @@ cudaError_t convert_f32_to_bf16(const float *x, void *y, int64_t n, cudaStream_t
   if (n <= 0) return cudaSuccess;
   int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
   f32_to_bf16_kernel<<<blocks, 256, 0, st>>>(x, reinterpret_cast<__nv_bfloat16 *>(y), n);
+  return cudaGetLastError();
+}
+
+
+// ===========================================================================
+// Geometry-bound operator: leg tables, weighted gather, adjoint scatter and
+// weight gradient (the differentiable beamformer and its CG solver).
+//
+// Leg tables hold, per (element, image point), the scaled FP64 leg as 32.32
+// fixed point with the A-scan column offset folded into the high word:
+//   TA[o][n] = (o*n_in*K << 32) + round(A(n,o) * 2^32) + delta
+//   TB[i][n] = (i*K << 32)      + round(B(n,i) * 2^32)
+// so TA + TB has the sample's element offset in its high word and the
+// fraction (shifted by delta) in its low word, exactly as in the tile kernel;
+// the same ambiguity band sends the rare boundary terms to the FP64 path, so
+// all three operators use the FP64 reference indices.
+// ===========================================================================
+
+namespace {
+
+constexpr uint32_t TAB_DELTA = 1u << 10;  // 2^-22 in 2^-32 units
+
+__global__ void legtab_kernel(const FastParams P, int64_t *__restrict__ TA, int64_t *__restrict__ TB,
+                              int *__restrict__ range) {
+  const int n_out = (P.method == RCA_ROWTX) ? P.Nr : P.Nt;
+  const int n_in = (P.method == RCA_ROWTX) ? P.Nt : P.Nr;
+  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = blockIdx.y;  // element: [0, n_out) outer, [n_out, n_out+n_in) inner
+  const bool active = n < P.No;
+  Pixel px;
+  pixel_of(P, active ? n : 0, px);
+  const bool outer = e < n_out;
+  const double L = outer ? A_mul_Fs(P, outer_leg(P, px, e)) : A_mul_Fs(P, inner_leg(P, px, e - n_out));
+  const bool ok = fabs(L) < 67108864.0;  // 2^26, as the tile kernel
+  const double f = floor(ok ? L : 0.0);
+  const int fl = (int)f;
+  const uint64_t frac = (uint64_t)__double2ull_rn((ok ? (L - f) : 0.0) * 4294967296.0);  // [0, 2^32]
+  const int64_t colk = outer ? (int64_t)e * n_in * P.K : (int64_t)(e - n_out) * P.K;
+  const int64_t v = ((colk + fl) << 32) + (int64_t)frac + (outer ? TAB_DELTA : 0);
+  if (active) {
+    if (outer) TA[(int64_t)e * P.No + n] = v;
+    else TB[(int64_t)(e - n_out) * P.No + n] = v;
+  }
+  // range[0..3]: min/max floor of outer legs, min/max of inner; [4]: overflow
+  int mn = __reduce_min_sync(0xffffffffu, active ? fl : INT_MAX);
+  int mx = __reduce_max_sync(0xffffffffu, active ? fl : INT_MIN);
+  bool bad = __any_sync(0xffffffffu, active && !ok);
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&range[outer ? 0 : 2], mn);
+    atomicMax(&range[outer ? 1 : 3], mx);
+    if (bad) atomicOr(&range[4], 1);
+  }
+}
+
+__global__ void legtab_classify_kernel(int *__restrict__ range, int64_t K, int64_t ny) {
+  // range[5] = 1: every non-ambiguous floor index lies in [0, K);
+  // range[6] = 1: element offsets fit 32 bits
+  const int64_t lo = (int64_t)range[0] + range[2], hi = (int64_t)range[1] + range[3];
+  range[5] = (range[4] == 0 && lo >= 0 && hi + 2 < K) ? 1 : 0;
+  range[6] = (range[4] == 0 && ny + hi + 256 < (int64_t(1) << 32) && lo > -(int64_t(1) << 30)) ? 1 : 0;
+}
+
+// Weighted gather Im[n] = sum_c w[c] Y[k(n,c), c] from the leg tables.
+template <class YT, bool WEIGHTED, bool CHECKED, int JC>
+__device__ __forceinline__ void tab_gather_body(const FastParams &P, const Pixel &px, const int64_t *TA,
+                                                const int64_t *TB, int64_t n, int n_out, int n_in,
+                                                float &acc_s, float &acc_c, unsigned int &oob) {
+  for (int i0 = 0; i0 < n_in; i0 += JC) {
+    const int jn = min(JC, n_in - i0);
+    uint64_t B64[JC];
+#pragma unroll
+    for (int j = 0; j < JC; j++) B64[j] = (j < jn) ? (uint64_t)__ldg(TB + (int64_t)(i0 + j) * P.No + n) : 0;
+    for (int o = 0; o < n_out; o++) {
+      const uint64_t A64 = (uint64_t)__ldg(TA + (int64_t)o * P.No + n);
+      float part = (jn == JC)
+                       ? chunk_terms<YT, WEIGHTED, CHECKED, true, JC>(P, px, B64, A64, (int64_t)o * n_in, o, i0,
+                                                                      JC, n_in, oob)
+                       : chunk_terms<YT, WEIGHTED, CHECKED, false, JC>(P, px, B64, A64, (int64_t)o * n_in, o,
+                                                                       i0, jn, n_in, oob);
+      neumaier(acc_s, acc_c, part);
+    }
+  }
+}
+
+template <class YT, bool WEIGHTED>
+__global__ void __launch_bounds__(256) tab_gather_kernel(const FastParams P, const int64_t *__restrict__ TA,
+                                                         const int64_t *__restrict__ TB,
+                                                         const int *__restrict__ range) {
+  const int n_out = (P.method == RCA_ROWTX) ? P.Nr : P.Nt;
+  const int n_in = (P.method == RCA_ROWTX) ? P.Nt : P.Nr;
+  const int64_t n_raw = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = n_raw < P.No;
+  const int64_t n = active ? n_raw : 0;
+  Pixel px;
+  pixel_of(P, n, px);
+  float acc_s = 0.0f, acc_c = 0.0f;
+  unsigned int oob = 0;
+  const bool exact_all = range[6] == 0;
+  if (exact_all) {
+    for (int o = 0; o < n_out; o++) {
+      for (int i0 = 0; i0 < n_in; i0 += 16)
+        neumaier(acc_s, acc_c, exact_partial<YT, WEIGHTED>(P, px, o, i0, min(16, n_in - i0), n_in, oob));
+    }
+  } else if (range[5]) {
+    tab_gather_body<YT, WEIGHTED, false, 16>(P, px, TA, TB, n, n_out, n_in, acc_s, acc_c, oob);
+  } else {
+    tab_gather_body<YT, WEIGHTED, true, 16>(P, px, TA, TB, n, n_out, n_in, acc_s, acc_c, oob);
+  }
+  if (active) P.Im[n] = acc_s + acc_c;
+  add_count(P.oob, active ? oob : 0u);
+}
+
+// The term's sample index for the column-owner kernels: returns -1 when the
+// term is out of bounds. Non-ambiguous in-range floor indices are final.
+__device__ __forceinline__ int tab_index(const FastParams &P, const Pixel &px, uint64_t s, int64_t colk, int o,
+                                         int i) {
+  const uint32_t lo = (uint32_t)s;
+  const int32_t kk = (int32_t)((uint32_t)(s >> 32) - (uint32_t)colk);
+  if (lo >= AMB_LO && kk >= 0 && kk < P.K) return kk;
+  int k;
+  return exact_index(P, px, o, i, k) ? k : -1;
+}
+
+// Column-owner adjoint and weight gradient. A CTA owns outer element o and
+// inner elements [i0, i0 + cw), loops over a share of the image points and
+//   adjoint: Ya[k(n,c), c] += w[c] * X[n]   (shared-memory histogram per column)
+//   wgrad:   dW[c] += G[n] * Y[k(n,c), c]  (per-thread partials, block reduction)
+template <bool ADJ, bool WG>
+__global__ void __launch_bounds__(256) tab_colowner_kernel(const FastParams P, const int64_t *__restrict__ TA,
+                                                           const int64_t *__restrict__ TB,
+                                                           const float *__restrict__ X, const float *__restrict__ G,
+                                                           float *__restrict__ Ya, float *__restrict__ dW, int cw,
+                                                           int splits) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float *hist = reinterpret_cast<float *>(smem_raw);  // [cw][K] (adjoint)
+  float *red = hist + (ADJ ? (size_t)cw * P.K : 0);   // [cw][warps] (wgrad)
+  const int n_in = (P.method == RCA_ROWTX) ? P.Nt : P.Nr;
+  const int o = blockIdx.x;
+  const int i0 = blockIdx.y * cw;
+  const int jn = min(cw, n_in - i0);
+  const int split = blockIdx.z;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const float *Yf = reinterpret_cast<const float *>(P.Y);
+  if (ADJ) {
+    for (int64_t q = tid; q < (int64_t)jn * P.K; q += nthr) hist[q] = 0.0f;
+    __syncthreads();
+  }
+  float wsum[16];
+#pragma unroll
+  for (int j = 0; j < 16; j++) wsum[j] = 0.0f;
+  float wc[16];
+#pragma unroll
+  for (int j = 0; j < 16; j++) wc[j] = (ADJ && j < jn) ? (P.w ? __ldg(P.w + (int64_t)o * n_in + i0 + j) : 1.0f) : 0.0f;
+  const int64_t per = (P.No + splits - 1) / splits;
+  const int64_t n0 = (int64_t)split * per, n1 = min(P.No, n0 + per);
+  for (int64_t n = n0 + tid; n < n1; n += nthr) {
+    Pixel px;
+    pixel_of(P, n, px);
+    const uint64_t A64 = (uint64_t)__ldg(TA + (int64_t)o * P.No + n);
+    const float xn = ADJ ? __ldg(X + n) : 0.0f;
+    const float gn = WG ? __ldg(G + n) : 0.0f;
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      if (j < jn) {
+        const int i = i0 + j;
+        const int64_t colk = ((int64_t)o * n_in + i) * P.K;
+        const uint64_t s = A64 + (uint64_t)__ldg(TB + (int64_t)i * P.No + n);
+        const int k = tab_index(P, px, s, colk, o, i);
+        if (k >= 0) {
+          if (ADJ) atomicAdd(hist + (int64_t)j * P.K + k, wc[j] * xn);
+          if (WG) wsum[j] = fmaf(gn, __ldg(Yf + colk + k), wsum[j]);
+        }
+      }
+    }
+  }
+  if (ADJ) {
+    __syncthreads();
+    for (int j = 0; j < jn; j++) {
+      float *dst = Ya + ((int64_t)o * n_in + i0 + j) * P.K;
+      for (int64_t k = tid; k < P.K; k += nthr) {
+        const float v = hist[(int64_t)j * P.K + k];
+        if (splits == 1) dst[k] = v;
+        else if (v != 0.0f) atomicAdd(dst + k, v);
+      }
+    }
+  }
+  if (WG) {
+    const int lane = tid & 31, warp = tid >> 5, nw = nthr >> 5;
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      float v = wsum[j];
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      if (lane == 0 && j < jn) red[j * nw + warp] = v;
+    }
+    __syncthreads();
+    if (tid < jn) {
+      float v = 0.0f;
+      for (int w = 0; w < nw; w++) v += red[tid * nw + w];
+      atomicAdd(dW + (int64_t)o * n_in + i0 + tid, v);
+    }
+  }
+}
+
+}  // namespace
+
+cudaError_t build_leg_tables(const FastParams &P, int64_t *TA, int64_t *TB, int *range, cudaStream_t st) {
+  const int n_out = (P.method == RCA_ROWTX) ? P.Nr : P.Nt;
+  const int n_in = (P.method == RCA_ROWTX) ? P.Nt : P.Nr;
+  const int init[7] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN, 0, 0, 0};
+  cudaError_t e = cudaMemcpyAsync(range, init, sizeof(init), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return e;
+  if (P.No > 0) {
+    dim3 grid((unsigned)((P.No + 255) / 256), (unsigned)(n_out + n_in));
+    legtab_kernel<<<grid, 256, 0, st>>>(P, TA, TB, range);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  legtab_classify_kernel<<<1, 1, 0, st>>>(range, P.K, (int64_t)n_out * n_in * P.K);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tab_gather(const FastParams &P, const int64_t *TA, const int64_t *TB, const int *range,
+                              cudaStream_t st) {
+  if (P.No <= 0) return cudaSuccess;
+  const unsigned g = (unsigned)((P.No + 255) / 256);
+  if (P.w) tab_gather_kernel<float, true><<<g, 256, 0, st>>>(P, TA, TB, range);
+  else tab_gather_kernel<float, false><<<g, 256, 0, st>>>(P, TA, TB, range);
+  return cudaGetLastError();
+}
+
+int colowner_width(int64_t K, int n_in) {
+  int cw = 16;
+  while (cw > 1 && (size_t)cw * K * 4 > 100 * 1024) cw >>= 1;
+  return std::min(cw, n_in);
+}
+
+cudaError_t launch_tab_colowner(const FastParams &P, const int64_t *TA, const int64_t *TB, const float *X,
+                                const float *G, float *Ya, float *dW, bool adj, bool wg, int sm_count,
+                                cudaStream_t st) {
+  const int n_out = (P.method == RCA_ROWTX) ? P.Nr : P.Nt;
+  const int n_in = (P.method == RCA_ROWTX) ? P.Nt : P.Nr;
+  if (n_out == 0 || n_in == 0) return cudaSuccess;
+  int cw = adj ? colowner_width(P.K, n_in) : std::min(16, n_in);
+  if (adj && (size_t)cw * P.K * 4 > 200 * 1024) return cudaErrorInvalidValue;  // A-scans too long for the histogram
+  const int groups = (n_in + cw - 1) / cw;
+  const int64_t ctas = (int64_t)n_out * groups;
+  int splits = (int)std::max<int64_t>(1, std::min<int64_t>(64, (4 * (int64_t)sm_count + ctas - 1) / ctas));
+  if (P.No < 4096) splits = 1;
+  const size_t smem = (adj ? (size_t)cw * P.K * 4 : 0) + (wg ? 16 * 8 * 4 : 0);
+  dim3 grid((unsigned)n_out, (unsigned)groups, (unsigned)splits);
+  cudaError_t e;
+  if (adj && wg) {
+    e = cudaFuncSetAttribute(tab_colowner_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) tab_colowner_kernel<true, true><<<grid, 256, smem, st>>>(P, TA, TB, X, G, Ya, dW, cw, splits);
+  } else if (adj) {
+    e = cudaFuncSetAttribute(tab_colowner_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) tab_colowner_kernel<true, false><<<grid, 256, smem, st>>>(P, TA, TB, X, G, Ya, dW, cw, splits);
+  } else {
+    e = cudaFuncSetAttribute(tab_colowner_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) tab_colowner_kernel<false, true><<<grid, 256, smem, st>>>(P, TA, TB, X, G, Ya, dW, cw, splits);
+  }
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
 

@@ -25,6 +25,7 @@ struct FastParams {
   // image tiling: point n = s*n_fast + f
   int64_t n_fast, n_slow;
   int tile_f, tile_s, wf;  // tile extents; warp lanes along the fast axis
+  int jc;                  // inner elements per register chunk: 8 or 16
   int64_t slow_tile0, slow_tile1;  // slow-tile range of this launch
   int64_t no0, no1;                // point range (SAFT launches)
 };
@@ -32,5 +33,17 @@ struct FastParams {
 size_t fast_smem_bytes(const FastParams &P, int nthr);
 cudaError_t launch_fast(const FastParams &P, bool bf16, cudaStream_t st);
 cudaError_t convert_f32_to_bf16(const float *x, void *y, int64_t n, cudaStream_t st);
+
+// Geometry-bound operator (leg tables; FP32 samples).
+// range: 7 ints of device scratch written by build_leg_tables.
+cudaError_t build_leg_tables(const FastParams &P, int64_t *TA, int64_t *TB, int *range, cudaStream_t st);
+cudaError_t launch_tab_gather(const FastParams &P, const int64_t *TA, const int64_t *TB, const int *range,
+                              cudaStream_t st);
+// Adjoint scatter (Ya must be zero when splits > 1; the launcher zeroes nothing)
+// and/or weight gradient (dW accumulated atomically: zero it first).
+cudaError_t launch_tab_colowner(const FastParams &P, const int64_t *TA, const int64_t *TB, const float *X,
+                                const float *G, float *Ya, float *dW, bool adj, bool wg, int sm_count,
+                                cudaStream_t st);
+int colowner_width(int64_t K, int n_in);
 
 }  // namespace dream

@@ -218,3 +218,22 @@ def rca_scene(seed: int = 2, n_cols: int = 128, n_rows: int = 128, K: int = 4096
     Ro = grid_xyz(nx, ny, nz, (-19.0, 19.0), (-19.0, 19.0), z_rng)
     return Scene(np.asfortranarray(Y), G_col, G_row, Ro, dt, np.zeros((1, 1), order="F"),
                  cp, method, (nx, ny, nz), {"scatterers": S, "amp": amp})
+
+
+def cg_scene(seed: int = 4, n_el: int = 32, K: int = 2048, nx: int = 256, nz: int = 256,
+             density: float = 0.01, dt: float = 0.04, cp: float = 1500.0, pitch: float = 0.5,
+             x_rng=(-8.0, 8.0), z_rng=(5.0, 37.0)):
+    """Model-based reconstruction scene: a 32 x 32 TFM array, K = 2048, and a
+    seeded sparse reflectivity image on a 256 x 256 grid (``density`` of the
+    points nonzero, values N(0, 1)). The A-scans are synthesised by the
+    adjoint (scatter) operator, so this returns the geometry and the image;
+    ``Y`` is left empty (K x 0)."""
+    rng = np.random.default_rng(seed)
+    G = linear_array(n_el, pitch)
+    Ro = grid_xz(nx, nz, x_rng, z_rng)
+    x = np.zeros(Ro.shape[0])
+    nnz = max(1, int(round(density * x.size)))
+    idx = rng.choice(x.size, nnz, replace=False)
+    x[idx] = rng.normal(0.0, 1.0, nnz)
+    return Scene(np.zeros((K, 0), order="F"), G, G.copy(order="F"), Ro, dt, np.zeros((1, 1), order="F"),
+                 cp, "tfm", (nx, nz), {"reflectivity": x})

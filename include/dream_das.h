@@ -190,6 +190,10 @@ int dream_das_set_grid_hint(dream_das_plan *plan, int64_t n_fast);
 int dream_das_set_tile(dream_das_plan *plan, int tile_f, int tile_s);
 int dream_das_get_tile(const dream_das_plan *plan, int *tile_f, int *tile_s);
 
+/* Inner elements per register chunk of the F32_STORE / BF16_STORE kernels:
+ * 8 or 16 (0 = automatic, 16). Used by the autotuner. */
+int dream_das_set_chunk(dream_das_plan *plan, int jc);
+
 /*
  * Weighted DAS, the forward operator of the differentiable beamformer:
  *   Im[n] = sum over A-scan columns c of w[c] * Y[k(n, c), c]
@@ -202,6 +206,34 @@ int dream_das_weighted_run_device(dream_das_plan *plan, const void *dY, const vo
                                   const void *dGt, const void *dGr, double dt, int delay_type,
                                   const void *ddelay, double cp, const float *dW, float *dIm,
                                   unsigned long long *d_oob, void *stream);
+
+/*
+ * Geometry-bound operator of the differentiable beamformer (F32_STORE plans;
+ * FP32 A-scans, images and weights). No reference counterpart: DREAM has no
+ * adjoint; its explicit DAS matrix example (examples/model_based_example.m:
+ * 381-456) is what this replaces.
+ *
+ * dream_das_bind_geometry computes the FP64 leg tables once (plan-owned
+ * device memory, (Nt+Nr)*No*8 bytes) and keeps the device pointers dRo, dGt,
+ * dGr, ddelay, which must stay valid while bound. With the A-scan column
+ * index c and the FP64 reference sample index k(n, c):
+ *   forward  Im[n]    = sum_c w[c] * Y[k(n,c), c]          (w NULL: all ones)
+ *   adjoint  Ya[k, c] = w[c] * sum_{n: k(n,c)=k} X[n]       (Ya overwritten)
+ *   wgrad    dW[c]    = sum_n G[n] * Y[k(n,c), c]           (dW overwritten)
+ *   backward adjoint(G, w) into dYg and wgrad(G, Y) into dWg in one pass
+ * All are asynchronous on `stream`; forward adds out-of-bounds terms to
+ * d_oob when it is not NULL.
+ */
+int dream_das_bind_geometry(dream_das_plan *plan, const void *dRo, const void *dGt, const void *dGr,
+                            double dt, int delay_type, const void *ddelay, double cp, void *stream);
+int dream_das_op_forward(dream_das_plan *plan, const float *dY, const float *dW, float *dIm,
+                         unsigned long long *d_oob, void *stream);
+int dream_das_op_adjoint(dream_das_plan *plan, const float *dX, const float *dW, float *dYa,
+                         void *stream);
+int dream_das_op_wgrad(dream_das_plan *plan, const float *dG, const float *dY, float *dWgrad,
+                       void *stream);
+int dream_das_op_backward(dream_das_plan *plan, const float *dG, const float *dY, const float *dW,
+                          float *dYgrad, float *dWgrad, void *stream);
 
 /* Requests cancellation: running and later calls return DREAM_ERR_CANCELLED
  * between launches until dream_das_set_running is called. */
