@@ -59,6 +59,11 @@ SIGNATURES = {
     "dream_das_op_adjoint": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "dream_das_op_wgrad": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "dream_das_op_backward": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "dream_das_batch_create": (_i, [_pp, _vp, _i, _i, _i]),
+    "dream_das_batch_run": (_i, [_vp, _vp, _vp]),
+    "dream_das_batch_items": (_i64, [_vp]),
+    "dream_das_batch_grid": (_i, [_vp]),
+    "dream_das_batch_destroy": (None, [_vp]),
     "dream_das_cancel": (None, [_vp]),
     "dream_das_set_running": (None, [_vp]),
 }

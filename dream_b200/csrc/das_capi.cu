@@ -10,8 +10,10 @@
 #include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/dream_das.h"
 #include "das_fast.h"
@@ -613,6 +615,174 @@ int dream_das_op_backward(dream_das_plan *p, const float *dG, const float *dY, c
   std::lock_guard<std::mutex> lk(p->mu);
   DeviceGuard g(p->device);
   return op_colowner(p, dG, dG, dY, dW, dYgrad, dWgrad, true, true, (cudaStream_t)stream);
+}
+
+}  // extern "C"
+
+struct dream_das_batch {
+  int device = 0;
+  bool bf16 = false;
+  int n_frames = 0;
+  int64_t n_items = 0;
+  size_t smem = 0;
+  int grid = 0;
+  DevBuf bFrames, bItems, bCtr;
+  std::vector<FastParams> frames;  // host copy (oob pointer patched per run)
+  unsigned long long *last_oob = nullptr;
+  std::mutex mu;
+};
+
+extern "C" {
+
+int dream_das_batch_create(dream_das_batch **out, const dream_das_frame *fr, int n_frames, int precision, int device) {
+  if (out == nullptr || (fr == nullptr && n_frames > 0) || n_frames < 0) return fail(DREAM_ERR_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  if (precision != DREAM_PREC_F32_STORE && precision != DREAM_PREC_BF16_STORE)
+    return fail(DREAM_ERR_UNSUPPORTED, "batches use F32_STORE or BF16_STORE");
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
+  if (device < 0 || device >= ndev) return fail(DREAM_ERR_ARGUMENT, "invalid CUDA device ordinal");
+  DeviceGuard g(device);
+  auto *b = new dream_das_batch();
+  b->device = device;
+  b->bf16 = precision == DREAM_PREC_BF16_STORE;
+  b->n_frames = n_frames;
+  struct Group {
+    double cost;
+    int f;
+    int64_t tf, ts;
+  };
+  std::vector<Group> groups;
+  for (int f = 0; f < n_frames; f++) {
+    const dream_das_frame &d = fr[f];
+    int r = check_common(d.das_type, d.a_scan_len, d.No, d.num_t_elements, d.num_r_elements, DREAM_PREC_F32_STORE);
+    if (!r && (d.das_type == DREAM_DAS_SAFT || d.num_r_elements == 0))
+      r = fail(DREAM_ERR_UNSUPPORTED, "batch frames must be TFM or RCA");
+    if (!r && d.das_type >= DREAM_DAS_RCA_COLTX) r = check_rca_edges(d.num_t_elements, d.num_r_elements);
+    if (!r && (d.n_fast < 0 || (d.n_fast > 0 && d.No % d.n_fast)))
+      r = fail(DREAM_ERR_ARGUMENT, "grid hint must divide the number of image points");
+    if (!r && (d.tile_f || d.tile_s) &&
+        (d.tile_f * d.tile_s != 128 || (d.n_fast > 0 ? (d.tile_f % 8 || d.tile_s % 4) : d.tile_s != 1)))
+      r = fail(DREAM_ERR_ARGUMENT, "invalid frame tile (tile_f * tile_s must be 128)");
+    if (!r && d.jc != 0 && d.jc != 8 && d.jc != 16) r = fail(DREAM_ERR_ARGUMENT, "chunk must be 0, 8 or 16");
+    if (!r && d.No > 0 && d.a_scan_len > 0 &&
+        (d.Y == nullptr || d.Ro == nullptr || d.Gt == nullptr || d.Gr == nullptr || d.delay == nullptr || d.Im == nullptr))
+      r = fail(DREAM_ERR_ARGUMENT, "NULL frame pointer");
+    if (r) {
+      dream_das_batch_destroy(b);
+      return r;
+    }
+    FastParams F;
+    memset(&F, 0, sizeof(F));
+    F.method = d.das_type;
+    F.Y = d.Y;
+    F.K = d.a_scan_len;
+    F.Ro = d.Ro;
+    F.No = d.No;
+    F.Gt = d.Gt;
+    F.Nt = (int)d.num_t_elements;
+    F.Gr = d.Gr;
+    F.Nr = (int)d.num_r_elements;
+    F.delay = d.delay;
+    F.delay_multi = d.delay_type == DREAM_DELAY_MULTIPLE;
+    Consts64 c = constants_f64(d.dt, d.cp, 0.0);
+    F.Fs = c.Fs;
+    F.ocp = c.ocp;
+    F.Im = d.Im;
+    if (d.n_fast > 0) {
+      F.n_fast = d.n_fast;
+      F.n_slow = d.No / d.n_fast;
+      F.wf = 8;
+      F.tile_f = d.tile_f ? d.tile_f : 16;
+      F.tile_s = d.tile_s ? d.tile_s : 8;
+    } else {
+      F.n_fast = d.No;
+      F.n_slow = 1;
+      F.wf = 32;
+      F.tile_f = 128;
+      F.tile_s = 1;
+    }
+    F.jc = d.jc ? d.jc : 16;
+    b->smem = std::max(b->smem, fast_smem_bytes(F, 128));
+    b->frames.push_back(F);
+    if (d.No > 0 && d.a_scan_len > 0) {
+      const int64_t tf = (F.n_fast + F.tile_f - 1) / F.tile_f, ts = (F.n_slow + F.tile_s - 1) / F.tile_s;
+      groups.push_back({(double)d.num_t_elements * d.num_r_elements, f, tf, ts});
+    }
+  }
+  if (b->smem > 220 * 1024) {
+    dream_das_batch_destroy(b);
+    return fail(DREAM_ERR_UNSUPPORTED, "a frame has too many outer elements for the batch kernel");
+  }
+  // largest per-tile cost first: the queue drains big tiles before small ones
+  std::stable_sort(groups.begin(), groups.end(), [](const Group &a, const Group &c) { return a.cost > c.cost; });
+  std::vector<int4> items;
+  for (const Group &gr : groups)
+    for (int64_t ts = 0; ts < gr.ts; ts++)
+      for (int64_t tf = 0; tf < gr.tf; tf++) items.push_back(make_int4(gr.f, (int)tf, (int)ts, 0));
+  b->n_items = (int64_t)items.size();
+  if (b->n_items > INT32_MAX) {
+    dream_das_batch_destroy(b);
+    return fail(DREAM_ERR_ARGUMENT, "too many tiles in one batch");
+  }
+  int r;
+  if ((r = b->bFrames.ensure(std::max<size_t>(1, b->frames.size()) * sizeof(FastParams))) ||
+      (r = b->bItems.ensure(std::max<size_t>(1, items.size()) * sizeof(int4))) || (r = b->bCtr.ensure(sizeof(int)))) {
+    dream_das_batch_destroy(b);
+    return r;
+  }
+  if (!items.empty()) {
+    e = cudaMemcpy(b->bItems.p, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      dream_das_batch_destroy(b);
+      return cuda_fail(e, "copying the work list");
+    }
+  }
+  int per_sm = batch_prepare(std::max<size_t>(b->smem, 1024), b->bf16);
+  if (per_sm <= 0) {
+    dream_das_batch_destroy(b);
+    return fail(DREAM_ERR_CUDA, "batch kernel does not fit on an SM");
+  }
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  b->grid = (int)std::min<int64_t>((int64_t)sms * per_sm, std::max<int64_t>(1, b->n_items));
+  b->last_oob = (unsigned long long *)1;  // force the first upload
+  *out = b;
+  return 0;
+}
+
+int dream_das_batch_run(dream_das_batch *b, unsigned long long *d_oob, void *stream) {
+  if (b == nullptr) return fail(DREAM_ERR_ARGUMENT, "batch is NULL");
+  std::lock_guard<std::mutex> lk(b->mu);
+  DeviceGuard g(b->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (d_oob != b->last_oob) {
+    // the frame table holds the counter pointer: upload it when it changes
+    for (auto &F : b->frames) F.oob = d_oob;
+    CU(cudaMemcpyAsync(b->bFrames.p, b->frames.data(), b->frames.size() * sizeof(FastParams),
+                       cudaMemcpyHostToDevice, st));
+    CU(cudaStreamSynchronize(st));
+    b->last_oob = d_oob;
+  }
+  CU(launch_batch((const FastParams *)b->bFrames.p, (const int4 *)b->bItems.p, (int)b->n_items, (int *)b->bCtr.p,
+                  std::max<size_t>(b->smem, 1024), b->bf16, b->grid, st));
+  return 0;
+}
+
+int64_t dream_das_batch_items(const dream_das_batch *b) { return b ? b->n_items : -1; }
+
+int dream_das_batch_grid(const dream_das_batch *b) { return b ? b->grid : -1; }
+
+void dream_das_batch_destroy(dream_das_batch *b) {
+  if (b == nullptr) return;
+  {
+    DeviceGuard g(b->device);
+    b->bFrames.release();
+    b->bItems.release();
+    b->bCtr.release();
+  }
+  delete b;
 }
 
 int dream_das_weighted_run_device(dream_das_plan *p, const void *dY, const void *dRo, const void *dGt,

@@ -282,9 +282,12 @@ __device__ __forceinline__ void tile_loop(const FastParams &P, const Pixel &px, 
 
 }  // namespace
 
+// One tile of image points (tile indices tfi along the fast axis, tsi along
+// the slow axis) with the frame described by P; smem_raw holds the tile's
+// shared arrays (fast_smem_bytes). Called by the one-frame kernel and by the
+// persistent batch kernel.
 template <class YT, bool WEIGHTED, int JC>
-__global__ void __launch_bounds__(256) das_fast_kernel(const FastParams P) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void fast_tile(const FastParams &P, int64_t tfi, int64_t tsi, unsigned char *smem_raw) {
   const int tid = threadIdx.x;
   const int nthr = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5;
@@ -304,7 +307,6 @@ __global__ void __launch_bounds__(256) das_fast_kernel(const FastParams P) {
   const int lf = lane % P.wf, ls = lane / P.wf;
   const int warps_f = P.tile_f / P.wf;
   const int wfi = warp % warps_f, wsi = warp / warps_f;
-  const int64_t tfi = blockIdx.x, tsi = (int64_t)blockIdx.y + P.slow_tile0;
   const int64_t f = tfi * P.tile_f + wfi * P.wf + lf;
   const int64_t s = tsi * P.tile_s + wsi * (32 / P.wf) + ls;
   const bool active = f < P.n_fast && s < P.n_slow;
@@ -402,6 +404,37 @@ __global__ void __launch_bounds__(256) das_fast_kernel(const FastParams P) {
   add_count(P.oob, active ? oob : 0u);
 }
 
+template <class YT, bool WEIGHTED, int JC>
+__global__ void __launch_bounds__(256) das_fast_kernel(const FastParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  fast_tile<YT, WEIGHTED, JC>(P, blockIdx.x, (int64_t)blockIdx.y + P.slow_tile0, smem_raw);
+}
+
+// Persistent batch kernel: CTAs take (frame, tile) work items from a queue
+// (items sorted by decreasing cost on the host) until it is empty. The frame
+// descriptor is staged in shared memory; every frame's tile has blockDim.x
+// points. ctr must be zero at launch (the batch run resets it).
+template <class YT>
+__global__ void __launch_bounds__(128) das_batch_kernel(const FastParams *__restrict__ frames,
+                                                        const int4 *__restrict__ items, int n_items,
+                                                        int *__restrict__ ctr) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ FastParams sP;
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(ctr, 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= n_items) break;
+    const int4 w = items[it];
+    if (threadIdx.x == 0) sP = frames[w.x];
+    __syncthreads();
+    if (sP.jc == 8) fast_tile<YT, false, 8>(sP, w.y, w.z, smem_raw);
+    else fast_tile<YT, false, 16>(sP, w.y, w.z, smem_raw);
+    __syncthreads();
+  }
+}
+
 // SAFT: one leg per term, t_dp = 2*(leg + delay); the FP64 index is computed
 // per term (each term has its own element), samples from FP32/BF16 storage.
 template <class YT, bool WEIGHTED>
@@ -475,6 +508,34 @@ cudaError_t launch_fast(const FastParams &P, bool bf16, cudaStream_t st) {
   const bool W = P.w != nullptr;
   if (bf16) return W ? launch_fast_t<__nv_bfloat16, true>(P, st) : launch_fast_t<__nv_bfloat16, false>(P, st);
   return W ? launch_fast_t<float, true>(P, st) : launch_fast_t<float, false>(P, st);
+}
+
+// Stream operations only (memset + launch), so a batch run can be captured
+// in a CUDA graph; the kernel attribute is set once by batch_prepare.
+cudaError_t launch_batch(const FastParams *frames, const int4 *items, int n_items, int *ctr, size_t smem, bool bf16,
+                         int grid, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(ctr, 0, sizeof(int), st);
+  if (e != cudaSuccess || n_items == 0) return e;
+  if (bf16) das_batch_kernel<__nv_bfloat16><<<grid, 128, smem, st>>>(frames, items, n_items, ctr);
+  else das_batch_kernel<float><<<grid, 128, smem, st>>>(frames, items, n_items, ctr);
+  return cudaGetLastError();
+}
+
+// Sets the dynamic shared-memory limit; returns resident CTAs per SM (0 on error).
+int batch_prepare(size_t smem, bool bf16) {
+  int n = 0;
+  if (bf16) {
+    if (cudaFuncSetAttribute(das_batch_kernel<__nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+      return 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, das_batch_kernel<__nv_bfloat16>, 128, smem);
+  } else {
+    if (cudaFuncSetAttribute(das_batch_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+      return 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, das_batch_kernel<float>, 128, smem);
+  }
+  return n;
 }
 
 cudaError_t convert_f32_to_bf16(const float *x, void *y, int64_t n, cudaStream_t st) {

@@ -46,4 +46,10 @@ cudaError_t launch_tab_colowner(const FastParams &P, const int64_t *TA, const in
                                 cudaStream_t st);
 int colowner_width(int64_t K, int n_in);
 
+// Persistent batch launch over (frame, tile_f index, tile_s index) items
+// (int4: frame, tfi, tsi, unused); resets the queue counter *ctr first.
+cudaError_t launch_batch(const FastParams *frames, const int4 *items, int n_items, int *ctr, size_t smem, bool bf16,
+                         int grid, cudaStream_t st);
+int batch_prepare(size_t smem, bool bf16);
+
 }  // namespace dream

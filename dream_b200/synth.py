@@ -237,3 +237,52 @@ def cg_scene(seed: int = 4, n_el: int = 32, K: int = 2048, nx: int = 256, nz: in
     x[idx] = rng.normal(0.0, 1.0, nnz)
     return Scene(np.zeros((K, 0), order="F"), G, G.copy(order="F"), Ro, dt, np.zeros((1, 1), order="F"),
                  cp, "tfm", (nx, nz), {"reflectivity": x})
+
+
+def batch_specs(seed: int = 7, n_frames: int = 48):
+    """Uneven frames for batched beamforming: elements per frame from
+    {16, 32, 64, 128} (tx = rx), A-scan length K ~ U{1024..4096}, cp ~
+    U[1450, 1550] m/s, square grids with a side ~ U{64..512}; dt = 0.04 us.
+    The imaged depth follows K so most paths fit in the A-scan."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_frames):
+        n_el = int(rng.choice([16, 32, 64, 128]))
+        K = int(rng.integers(1024, 4097))
+        cp = float(rng.uniform(1450.0, 1550.0))
+        side = int(rng.integers(64, 513))
+        out.append(dict(n_el=n_el, K=K, cp=cp, side=side, dt=0.04, seed=int(rng.integers(1 << 30))))
+    return out
+
+
+def tfm_frame_torch(spec: dict, device="cuda", n_scat: int = 10, noise: float = 0.01):
+    """One batch frame with its A-scans synthesised on the GPU (torch): seeded
+    point scatterers with the 5 MHz Gaussian-windowed sine plus N(0, noise).
+    Returns (Y column-major FP32 (K, n_el^2) on the device, G, Ro, dt, cp)."""
+    import torch
+    rng = np.random.default_rng(spec["seed"])
+    n_el, K, cp, side, dt = spec["n_el"], spec["K"], spec["cp"], spec["side"], spec["dt"]
+    v = cp / 1000.0
+    z_max = min(50.0, 0.35 * K * dt * v)
+    x_half = min(20.0, 0.5 * z_max)
+    G = linear_array(n_el, 0.5)
+    Ro = grid_xz(side, side, (-x_half, x_half), (2.0, z_max))
+    S = np.stack([rng.uniform(-0.6 * x_half, 0.6 * x_half, n_scat), np.zeros(n_scat),
+                  rng.uniform(0.25 * z_max, 0.9 * z_max, n_scat)], axis=1)
+    amp = rng.uniform(0.5, 1.0, n_scat)
+    d = torch.from_numpy(_dist(G, S)).to(device)                       # (n_el, S)
+    t = ((d[:, None, :] + d[None, :, :]) / v).reshape(n_el * n_el, n_scat)  # (C, S)
+    C = n_el * n_el
+    gen = torch.Generator(device=device).manual_seed(spec["seed"])
+    Yc = torch.randn((C, K), generator=gen, device=device, dtype=torch.float32) * noise  # row c = column c
+    half = int(np.ceil(0.5 / dt)) + 1
+    offs = torch.arange(-half, half + 1, device=device, dtype=torch.float64)
+    k = torch.floor(t / dt)[..., None] + offs                           # (C, S, W)
+    tau = k * dt - t[..., None]
+    val = torch.from_numpy(amp).to(device)[None, :, None] * torch.exp(-tau * tau / 0.02) * torch.sin(
+        2.0 * np.pi * 5.0 * tau)
+    ok = (k >= 0) & (k < K)
+    cols = torch.arange(C, device=device, dtype=torch.float64)[:, None, None].expand_as(k)
+    flat = (cols * K + k)[ok].long()
+    Yc.view(-1).index_add_(0, flat, val[ok].float())
+    return Yc.t(), G, Ro, dt, cp

@@ -235,6 +235,47 @@ int dream_das_op_wgrad(dream_das_plan *plan, const float *dG, const float *dY, f
 int dream_das_op_backward(dream_das_plan *plan, const float *dG, const float *dY, const float *dW,
                           float *dYgrad, float *dWgrad, void *stream);
 
+/*
+ * Batched DAS: many frames of uneven element counts, A-scan lengths and
+ * image sizes in ONE persistent launch. No reference counterpart (the
+ * reference beamforms one frame per call); each frame has the meaning of
+ * one dream_das_run_device call on an F32_STORE / BF16_STORE plan.
+ * Pointers are device pointers that must stay valid while the batch exists;
+ * their contents may change between runs (a run reads them when it executes,
+ * so a captured CUDA graph of dream_das_batch_run can be replayed on new
+ * data). TFM and RCA methods; tile_f * tile_s must be 128 when given.
+ */
+typedef struct dream_das_frame {
+  int das_type;
+  int64_t a_scan_len;
+  int64_t No;
+  int64_t num_t_elements;
+  int64_t num_r_elements;
+  const void *Y;       /* K x C, FP32 (F32_STORE) or BF16 bits (BF16_STORE) */
+  const double *Ro;    /* No x 3 */
+  const double *Gt;    /* Nt x 3 */
+  const double *Gr;    /* Nr x 3 */
+  const double *delay; /* 1 or No values [us] */
+  int delay_type;
+  double dt, cp;
+  float *Im;           /* No */
+  int64_t n_fast;      /* grid hint, 0 = none */
+  int tile_f, tile_s;  /* 0, 0 = automatic */
+  int jc;              /* inner chunk 8 or 16, 0 = automatic */
+} dream_das_frame;
+
+typedef struct dream_das_batch dream_das_batch;
+
+int dream_das_batch_create(dream_das_batch **batch, const dream_das_frame *frames, int n_frames,
+                           int precision, int device);
+/* One persistent launch over all frames (queue reset + kernel, both stream
+ * operations: capturable). d_oob (may be NULL) accumulates out-of-bounds terms. */
+int dream_das_batch_run(dream_das_batch *batch, unsigned long long *d_oob, void *stream);
+/* Number of (frame, tile) work items and the persistent grid size. */
+int64_t dream_das_batch_items(const dream_das_batch *batch);
+int dream_das_batch_grid(const dream_das_batch *batch);
+void dream_das_batch_destroy(dream_das_batch *batch);
+
 /* Requests cancellation: running and later calls return DREAM_ERR_CANCELLED
  * between launches until dream_das_set_running is called. */
 void dream_das_cancel(dream_das_plan *plan);
