@@ -138,11 +138,15 @@ def tune(Y, Gt, Gr, Ro, dt, delay, cp, method="tfm", storage="f32", nthr=None, f
     return dict(best)
 
 
-def apply(plan, cfg) -> None:
-    """Sets a tuned configuration on a plan (its grid hint must match)."""
+def apply(plan, cfg, Ro) -> None:
+    """Sets a tuned configuration on a plan. The grid hint is taken from the
+    plan's own image points Ro (a cached entry is shared by every grid of its
+    bucket); the tile applies when the hinted/unhinted kind matches."""
     L = _lib.load()
-    _lib.check(L.dream_das_set_grid_hint(plan.handle, int(cfg["n_fast"])))
-    _lib.check(L.dream_das_set_tile(plan.handle, int(cfg["tile"][0]), int(cfg["tile"][1])))
+    h = grid_hint(Ro)
+    _lib.check(L.dream_das_set_grid_hint(plan.handle, h))
+    if (h > 0) == (int(cfg["n_fast"]) > 0):
+        _lib.check(L.dream_das_set_tile(plan.handle, int(cfg["tile"][0]), int(cfg["tile"][1])))
     _lib.check(L.dream_das_set_chunk(plan.handle, int(cfg["jc"])))
 
 

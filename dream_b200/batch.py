@@ -94,11 +94,13 @@ class DASBatch:
         if autotune:
             from .autotune import batch_config
             for f in self.frames:
+                if f.n_fast < 0:
+                    f.n_fast = grid_hint(f.Ro)  # always the frame's own grid
                 if f.tile is None or not f.jc:
-                    cfg = batch_config(f, storage)
-                    f.n_fast = cfg["n_fast"] if f.n_fast < 0 else f.n_fast
-                    f.tile = f.tile or tuple(cfg["tile"])
-                    f.jc = f.jc or cfg["jc"]
+                    cfg = batch_config(f, storage)  # shared by the frames of a bucket
+                    if (cfg["n_fast"] > 0) == (f.n_fast > 0):
+                        f.tile = f.tile or tuple(cfg["tile"])
+                        f.jc = f.jc or cfg["jc"]
         arr = (FrameStruct * max(1, len(self.frames)))()
         for i, f in enumerate(self.frames):
             if f.n_fast < 0:
