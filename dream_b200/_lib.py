@@ -64,6 +64,7 @@ SIGNATURES = {
     "dream_das_batch_items": (_i64, [_vp]),
     "dream_das_batch_grid": (_i, [_vp]),
     "dream_das_batch_destroy": (None, [_vp]),
+    "dream_das_batch_run_noalloc": (_i, [_vp, _i, _i, _i, _vp, _vp]),
     "dream_das_cancel": (None, [_vp]),
     "dream_das_set_running": (None, [_vp]),
 }

@@ -92,6 +92,8 @@ int status_from_oob(uint64_t oob, int err_level) {
 
 }  // namespace
 
+int dream::set_last_error(int code, const std::string &msg) { return fail(code, msg); }
+
 struct dream_das_plan {
   int das_type = 0;
   int64_t K = 0, No = 0, Nt = 0, Nr = 0;

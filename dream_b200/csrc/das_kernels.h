@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 namespace dream {
 
 // Per-call constants, computed on the host exactly as the restated reference
@@ -40,6 +42,10 @@ struct PlainLaunch {
 };
 
 cudaError_t launch_plain_f64(const PlainLaunch &L, cudaStream_t st);
+
+// Records msg as this host thread's last error (dream_das_last_error) and
+// returns code.
+int set_last_error(int code, const std::string &msg);
 cudaError_t launch_plain_f32(const PlainLaunch &L, cudaStream_t st);
 
 }  // namespace dream

@@ -276,6 +276,24 @@ int64_t dream_das_batch_items(const dream_das_batch *batch);
 int dream_das_batch_grid(const dream_das_batch *batch);
 void dream_das_batch_destroy(dream_das_batch *batch);
 
+/*
+ * Allocation-free batch run. No counterpart in the reference (DREAM always
+ * allocates its buffers). For callers that cannot call cudaMalloc -- device
+ * memory owned by another framework's pool or a budget fixed at start-up,
+ * real-time pipelines that forbid allocation after initialisation -- this
+ * runs the same persistent batch kernel as dream_das_batch_run without
+ * creating a batch object and without allocating: the work queue counter,
+ * frame table and tile list go to a 4 MiB device array inside this library
+ * (every GPU that loads the library holds it until exit). Batches needing
+ * more scratch are rejected with DREAM_ERR_ARGUMENT and a message.
+ * The first call on a device looks the array up (cudaGetSymbolAddress); make
+ * that first call before any stream capture. Calls share the array: calls
+ * that overlap on the GPU (other streams or threads) race; calls on one
+ * stream are ordered. Frames and d_oob as for dream_das_batch_create/_run.
+ */
+int dream_das_batch_run_noalloc(const dream_das_frame *frames, int n_frames, int precision,
+                                int device, unsigned long long *d_oob, void *stream);
+
 /* Requests cancellation: running and later calls return DREAM_ERR_CANCELLED
  * between launches until dream_das_set_running is called. */
 void dream_das_cancel(dream_das_plan *plan);
