@@ -247,6 +247,45 @@ def cg_bench(dev, iters: int = 30, reps: int = 3):
             "scatter_gsum_s": sums / t_s / 1e6}
 
 
+def rca_bench(dev, steps: int = 3):
+    """The RCA configuration: 128x128 row-column array, row transmit, K=4096,
+    128x128x256 grid (68.7e9 sums), A-scans stored in FP32 (268 MB, larger
+    than L2) and in BF16; plain FP32 for comparison. Device-resident inputs."""
+    import torch
+    from dream_b200 import _lib, synth
+    from dream_b200.beamformer import grid_hint
+    L = _lib.load()
+    Y, Gc, Gr_, Ro = synth.rca_frame_torch(device=dev)
+    f = lambda a, dt: torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=dt).T)).to(dev).t()
+    out = {"config": "RCA 128x128 row-tx, K=4096, 128x128x256 grid", "sums": int(Ro.shape[0]) * 128 * 128}
+    d_oob = torch.zeros(1, dtype=torch.int64, device=dev)
+    for name, prec in (("f32_store", _lib.PREC_F32_STORE), ("bf16_store", _lib.PREC_BF16_STORE),
+                       ("plain_f32", _lib.PREC_F32)):
+        geo = np.float32 if prec == _lib.PREC_F32 else np.float64
+        Gt_d, Gr_d, Ro_d, dl = f(Gc, geo), f(Gr_, geo), f(Ro, geo), f(np.zeros((1, 1)), geo)
+        Yd = Y.t().contiguous().to(torch.bfloat16).t() if prec == _lib.PREC_BF16_STORE else Y
+        Im = torch.empty(Ro.shape[0], device=dev, dtype=torch.float32)
+        plan = _lib.plan_create(_lib.RCA_ROWTX, 4096, Ro.shape[0], 128, 128, prec, dev.index)
+        if prec != _lib.PREC_F32:
+            _lib.check(L.dream_das_set_grid_hint(plan.handle, grid_hint(Ro)))
+        ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+        cast = (lambda v: float(np.float32(v))) if prec == _lib.PREC_F32 else float
+        args_ = (plan.handle, ptr(Yd), ptr(Ro_d), ptr(Gt_d), ptr(Gr_d), cast(0.025), _lib.DELAY_SINGLE, ptr(dl),
+                 cast(1480.0), ptr(Im), ptr(d_oob), ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+        _lib.check(L.dream_das_run_device_async(*args_))
+        torch.cuda.synchronize()
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            _lib.check(L.dream_das_run_device_async(*args_))
+        e.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(e) / steps
+        out[name] = {"ms_per_frame": ms, "gsum_s": out["sums"] / ms / 1e6}
+        del Yd
+    return out
+
+
 def batch_bench(dev, steps: int = 10, n_frames: int = 48):
     """48 uneven TFM frames (elements from {16,32,64,128}, K ~ U{1024..4096},
     cp ~ U[1450,1550], grids 64^2..512^2), FP32, one persistent launch captured
@@ -316,6 +355,7 @@ def main():
     d_oob = torch.zeros(1, dtype=torch.int64, device=dev)
     from dream_b200.beamformer import grid_hint
     hint = grid_hint(scene.Ro)
+    tuned = {}
 
     def variant(prec_code, steps, warmup):
         geo_dt = np.float32 if prec_code == _lib.PREC_F32 else np.float64
@@ -328,7 +368,11 @@ def main():
         Im = torch.empty(No, dtype=torch.float64 if prec_code == _lib.PREC_F64 else torch.float32, device=dev)
         plan = _lib.plan_create(_lib.TFM, K, No, Nt, Nr, prec_code, local)
         if prec_code in (_lib.PREC_F32_STORE, _lib.PREC_BF16_STORE):
-            _lib.check(L.dream_das_set_grid_hint(plan.handle, hint))
+            from dream_b200 import autotune
+            cfg = autotune.tune(Y, Gt, Gr, Ro, scene.dt, delay, scene.cp, "tfm",
+                                "bf16" if prec_code == _lib.PREC_BF16_STORE else "f32")
+            autotune.apply(plan, cfg, Ro)
+            tuned[prec_code] = cfg
         ptr = lambda t: ctypes.c_void_p(t.data_ptr())
         cast = (lambda v: float(np.float32(v))) if prec_code == _lib.PREC_F32 else float
         args_ = (plan.handle, ptr(Y), ptr(Ro), ptr(Gt), ptr(Gr), cast(scene.dt), _lib.DELAY_SINGLE,
@@ -415,6 +459,7 @@ def main():
 
     cg = cg_bench(dev)
     batched = batch_bench(dev)
+    rca = rca_bench(dev)
 
     if world > 1:
         dist.destroy_process_group()
@@ -445,6 +490,8 @@ def main():
                      "compulsory_hbm_frac": compulsory / (step_ms * 1e-3) / 1e9 / peak},
         "adjoint_cg": cg,
         "batched": batched,
+        "rca": rca,
+        "autotuned": {("bf16_store" if k == _lib.PREC_BF16_STORE else "f32_store"): v for k, v in tuned.items()},
         "gpu_launches": int(launches_h),
         "clocks": clk,
     }

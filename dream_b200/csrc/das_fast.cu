@@ -187,7 +187,7 @@ __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &p
   const int64_t K = P.K;
   float y[JC];
   uint32_t minlo = 0xffffffffu;
-  bool bad = false;
+  unsigned int oob_chunk = 0;
 #pragma unroll
   for (int j = 0; j < JC; j++) {
     y[j] = 0.0f;
@@ -197,11 +197,14 @@ __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &p
       const uint32_t off = (uint32_t)(s >> 32);
       minlo = min(minlo, lo);
       if (CHECKED) {
+        // Outside the ambiguity band the floor index is exact: [0, K) is in
+        // bounds, -1 means p in (-1, 0), i.e. sample 0 after truncation, and
+        // anything else is out of bounds.
         const int64_t col0 = (colbase + i0 + j) * K;
         const int32_t kk = (int32_t)(off - (uint32_t)col0);  // floor index, exact modulo 2^32
-        const bool in = kk >= 0 && kk < K;
-        bad |= !in;
-        if (in) y[j] = load_sample(Y + col0 + kk);
+        if (kk >= 0 && kk < K) y[j] = load_sample(Y + col0 + kk);
+        else if (kk == -1) y[j] = load_sample(Y + col0);
+        else oob_chunk++;
       } else {
         y[j] = load_sample(elem_addr(Y, off));
       }
@@ -228,7 +231,8 @@ __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &p
 #pragma unroll
     for (int j = 0; j < JC; j++) part += y[j];
   }
-  if (minlo < AMB_LO || bad) part = exact_partial<YT, WEIGHTED>(P, px, o, i0, jn, n_in, oob);
+  if (minlo < AMB_LO) part = exact_partial<YT, WEIGHTED>(P, px, o, i0, jn, n_in, oob);  // counts its own
+  else oob += oob_chunk;
   return part;
 }
 
@@ -655,14 +659,21 @@ __global__ void __launch_bounds__(256) tab_gather_kernel(const FastParams P, con
 }
 
 // The term's sample index for the column-owner kernels: returns -1 when the
-// term is out of bounds. Non-ambiguous in-range floor indices are final.
-__device__ __forceinline__ int tab_index(const FastParams &P, const Pixel &px, uint64_t s, int64_t colk, int o,
-                                         int i) {
-  const uint32_t lo = (uint32_t)s;
-  const int32_t kk = (int32_t)((uint32_t)(s >> 32) - (uint32_t)colk);
-  if (lo >= AMB_LO && kk >= 0 && kk < P.K) return kk;
+// term is out of bounds. Outside the ambiguity band the floor index decides
+// (-1 is p in (-1, 0): sample 0); inside it the FP64 index is recomputed, the
+// only place that needs the image point's coordinates.
+__device__ __noinline__ int tab_index_exact(const FastParams &P, int64_t n, int o, int i) {
+  Pixel px;
+  pixel_of(P, n, px);
   int k;
   return exact_index(P, px, o, i, k) ? k : -1;
+}
+
+__device__ __forceinline__ int tab_index(const FastParams &P, int64_t n, uint64_t s, int64_t colk, int o, int i) {
+  const uint32_t lo = (uint32_t)s;
+  const int32_t kk = (int32_t)((uint32_t)(s >> 32) - (uint32_t)colk);
+  if (lo >= AMB_LO) return (kk >= 0 && kk < P.K) ? kk : (kk == -1 ? 0 : -1);
+  return tab_index_exact(P, n, o, i);
 }
 
 // Column-owner adjoint and weight gradient. A CTA owns outer element o and
@@ -698,8 +709,6 @@ __global__ void __launch_bounds__(256) tab_colowner_kernel(const FastParams P, c
   const int64_t per = (P.No + splits - 1) / splits;
   const int64_t n0 = (int64_t)split * per, n1 = min(P.No, n0 + per);
   for (int64_t n = n0 + tid; n < n1; n += nthr) {
-    Pixel px;
-    pixel_of(P, n, px);
     const uint64_t A64 = (uint64_t)__ldg(TA + (int64_t)o * P.No + n);
     const float xn = ADJ ? __ldg(X + n) : 0.0f;
     const float gn = WG ? __ldg(G + n) : 0.0f;
@@ -709,7 +718,7 @@ __global__ void __launch_bounds__(256) tab_colowner_kernel(const FastParams P, c
         const int i = i0 + j;
         const int64_t colk = ((int64_t)o * n_in + i) * P.K;
         const uint64_t s = A64 + (uint64_t)__ldg(TB + (int64_t)i * P.No + n);
-        const int k = tab_index(P, px, s, colk, o, i);
+        const int k = tab_index(P, n, s, colk, o, i);
         if (k >= 0) {
           if (ADJ) atomicAdd(hist + (int64_t)j * P.K + k, wc[j] * xn);
           if (WG) wsum[j] = fmaf(gn, __ldg(Yf + colk + k), wsum[j]);

@@ -286,3 +286,40 @@ def tfm_frame_torch(spec: dict, device="cuda", n_scat: int = 10, noise: float = 
     flat = (cols * K + k)[ok].long()
     Yc.view(-1).index_add_(0, flat, val[ok].float())
     return Yc.t(), G, Ro, dt, cp
+
+
+def rca_frame_torch(seed: int = 2, n_cols: int = 128, n_rows: int = 128, K: int = 4096, nx: int = 128,
+                    ny: int = 128, nz: int = 256, n_scat: int = 20, dt: float = 0.025, cp: float = 1480.0,
+                    pitch: float = 0.3, method: str = "rca_rowtx", z_rng=(5.0, 35.0), noise: float = 0.005,
+                    device="cuda"):
+    """The RCA configuration with A-scans synthesised on the GPU (torch):
+    seeded point scatterers in a 38 x 38 x 30 mm volume, 6 MHz Gaussian-windowed
+    sine, N(0, noise). Returns (Y column-major FP32 (K, n_cols*n_rows) on the
+    device, G_col, G_row, Ro). Row-tx columns are row*n_cols + col."""
+    import torch
+    rng = np.random.default_rng(seed)
+    G_col, G_row = rca_arrays(n_cols, n_rows, pitch)
+    S = np.stack([rng.uniform(-19.0, 19.0, n_scat), rng.uniform(-19.0, 19.0, n_scat),
+                  rng.uniform(z_rng[0], z_rng[1], n_scat)], axis=1)
+    amp = rng.uniform(0.5, 1.0, n_scat)
+    v = cp / 1000.0
+    dc = torch.from_numpy(_stripe_dist_cols(G_col, G_row, S)).to(device)
+    dr = torch.from_numpy(_stripe_dist_rows(G_col, G_row, S)).to(device)
+    if method == "rca_rowtx":
+        t = ((dr[:, None, :] + dc[None, :, :]) / v).reshape(n_rows * n_cols, n_scat)
+    else:
+        t = ((dc[:, None, :] + dr[None, :, :]) / v).reshape(n_cols * n_rows, n_scat)
+    C = n_cols * n_rows
+    gen = torch.Generator(device=device).manual_seed(seed)
+    Yc = torch.randn((C, K), generator=gen, device=device, dtype=torch.float32) * noise
+    half = int(np.ceil(0.5 / dt)) + 1
+    offs = torch.arange(-half, half + 1, device=device, dtype=torch.float64)
+    k = torch.floor(t / dt)[..., None] + offs
+    tau = k * dt - t[..., None]
+    val = torch.from_numpy(amp).to(device)[None, :, None] * torch.exp(-tau * tau / 0.02) * torch.sin(
+        2.0 * np.pi * 6.0 * tau)
+    ok = (k >= 0) & (k < K)
+    cols = torch.arange(C, device=device, dtype=torch.float64)[:, None, None].expand_as(k)
+    Yc.view(-1).index_add_(0, (cols * K + k)[ok].long(), val[ok].float())
+    Ro = grid_xyz(nx, ny, nz, (-19.0, 19.0), (-19.0, 19.0), z_rng)
+    return Yc.t(), G_col, G_row, Ro
