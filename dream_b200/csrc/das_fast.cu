@@ -179,61 +179,82 @@ __device__ __noinline__ float exact_partial(const FastParams &P, const Pixel &px
 // issued unconditionally: in an in-bounds tile every floor index, ambiguous
 // or not, lies inside its A-scan. Ambiguity is tracked as the minimum
 // fraction word; a chunk whose minimum falls in the band is recomputed.
-template <class YT, bool WEIGHTED, bool CHECKED, bool FULL, int JC>
+template <class YT, bool WEIGHTED, bool CHECKED, bool FULL, int JC, int NO>
 __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &px, const uint64_t (&B64)[JC],
-                                             uint64_t A64, int64_t colbase, int o, int i0, int jn, int n_in,
+                                             const uint64_t (&A64)[NO], int o0, int i0, int jn, int n_in,
                                              unsigned int &oob) {
+  // NO outer elements x JC inner elements: all NO*JC gathers are issued before
+  // any (rare) call to the exact path, so they are in flight together.
   const YT *__restrict__ Y = reinterpret_cast<const YT *>(P.Y);
   const int64_t K = P.K;
-  float y[JC];
-  uint32_t minlo = 0xffffffffu;
-  unsigned int oob_chunk = 0;
+  float y[NO][JC];
+  uint32_t minlo[NO];
+  unsigned int oob_chunk[NO];
 #pragma unroll
-  for (int j = 0; j < JC; j++) {
-    y[j] = 0.0f;
-    if (FULL || j < jn) {
-      const uint64_t s = A64 + B64[j];
-      const uint32_t lo = (uint32_t)s;
-      const uint32_t off = (uint32_t)(s >> 32);
-      minlo = min(minlo, lo);
-      if (CHECKED) {
-        // Outside the ambiguity band the floor index is exact: [0, K) is in
-        // bounds, -1 means p in (-1, 0), i.e. sample 0 after truncation, and
-        // anything else is out of bounds.
-        const int64_t col0 = (colbase + i0 + j) * K;
-        const int32_t kk = (int32_t)(off - (uint32_t)col0);  // floor index, exact modulo 2^32
-        if (kk >= 0 && kk < K) y[j] = load_sample(Y + col0 + kk);
-        else if (kk == -1) y[j] = load_sample(Y + col0);
-        else oob_chunk++;
-      } else {
-        y[j] = load_sample(elem_addr(Y, off));
+  for (int q = 0; q < NO; q++) {
+    minlo[q] = 0xffffffffu;
+    oob_chunk[q] = 0;
+#pragma unroll
+    for (int j = 0; j < JC; j++) {
+      y[q][j] = 0.0f;
+      if (FULL || j < jn) {
+        const uint64_t s = A64[q] + B64[j];
+        const uint32_t lo = (uint32_t)s;
+        const uint32_t off = (uint32_t)(s >> 32);
+        minlo[q] = min(minlo[q], lo);
+        if (CHECKED) {
+          // Outside the ambiguity band the floor index is exact: [0, K) is in
+          // bounds, -1 means p in (-1, 0), i.e. sample 0 after truncation, and
+          // anything else is out of bounds.
+          const int64_t col0 = ((int64_t)(o0 + q) * n_in + i0 + j) * K;
+          const int32_t kk = (int32_t)(off - (uint32_t)col0);  // floor index, exact modulo 2^32
+          if (kk >= 0 && kk < K) y[q][j] = load_sample(Y + col0 + kk);
+          else if (kk == -1) y[q][j] = load_sample(Y + col0);
+          else oob_chunk[q]++;
+        } else {
+          y[q][j] = load_sample(elem_addr(Y, off));
+        }
       }
     }
   }
-  float part = 0.0f;
-  if (WEIGHTED) {
-    const float *w = P.w + colbase + i0;
-    if (FULL && ((reinterpret_cast<uintptr_t>(w) & 15) == 0)) {
+  float total = 0.0f;
+  float partq[NO];
 #pragma unroll
-      for (int j = 0; j < JC; j += 4) {
-        float4 w4 = __ldg(reinterpret_cast<const float4 *>(w + j));
-        part = fmaf(w4.x, y[j], part);
-        part = fmaf(w4.y, y[j + 1], part);
-        part = fmaf(w4.z, y[j + 2], part);
-        part = fmaf(w4.w, y[j + 3], part);
+  for (int q = 0; q < NO; q++) {
+    float part = 0.0f;
+    if (WEIGHTED) {
+      const float *w = P.w + (int64_t)(o0 + q) * n_in + i0;
+      if (FULL && ((reinterpret_cast<uintptr_t>(w) & 15) == 0)) {
+#pragma unroll
+        for (int j = 0; j < JC; j += 4) {
+          float4 w4 = __ldg(reinterpret_cast<const float4 *>(w + j));
+          part = fmaf(w4.x, y[q][j], part);
+          part = fmaf(w4.y, y[q][j + 1], part);
+          part = fmaf(w4.z, y[q][j + 2], part);
+          part = fmaf(w4.w, y[q][j + 3], part);
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < JC; j++)
+          if (FULL || j < jn) part = fmaf(__ldg(w + j), y[q][j], part);
       }
     } else {
 #pragma unroll
-      for (int j = 0; j < JC; j++)
-        if (FULL || j < jn) part = fmaf(__ldg(w + j), y[j], part);
+      for (int j = 0; j < JC; j++) part += y[q][j];
     }
-  } else {
-#pragma unroll
-    for (int j = 0; j < JC; j++) part += y[j];
+    partq[q] = part;
   }
-  if (minlo < AMB_LO) part = exact_partial<YT, WEIGHTED>(P, px, o, i0, jn, n_in, oob);  // counts its own
-  else oob += oob_chunk;
-  return part;
+#pragma unroll
+  for (int q = 0; q < NO; q++) {
+    if (minlo[q] < AMB_LO) {
+      // this outer element's partial is replaced by the exact one (which counts its own OOB)
+      partq[q] = exact_partial<YT, WEIGHTED>(P, px, o0 + q, i0, jn, n_in, oob);
+    } else {
+      oob += oob_chunk[q];
+    }
+    total += partq[q];
+  }
+  return total;
 }
 
 template <class YT, bool WEIGHTED, bool CHECKED, int JC>
@@ -261,24 +282,18 @@ __device__ __forceinline__ void tile_loop(const FastParams &P, const Pixel &px, 
       // compensation every two outer elements (32 terms)
       int o = 0;
       for (; o + 2 <= n_out; o += 2) {
-        const uint64_t A0 = ((uint64_t)S.arel[o * nthr + tid] << 8) + ((uint64_t)S.ahi[o] << 32);
-        const uint64_t A1 = ((uint64_t)S.arel[(o + 1) * nthr + tid] << 8) + ((uint64_t)S.ahi[o + 1] << 32);
-        float part = chunk_terms<YT, WEIGHTED, CHECKED, true, JC>(P, px, B64, A0, (int64_t)o * n_in, o, i0, JC,
-                                                             n_in, oob);
-        part += chunk_terms<YT, WEIGHTED, CHECKED, true, JC>(P, px, B64, A1, (int64_t)(o + 1) * n_in, o + 1, i0,
-                                                        JC, n_in, oob);
-        neumaier(acc_s, acc_c, part);
+        const uint64_t A2[2] = {((uint64_t)S.arel[o * nthr + tid] << 8) + ((uint64_t)S.ahi[o] << 32),
+                                ((uint64_t)S.arel[(o + 1) * nthr + tid] << 8) + ((uint64_t)S.ahi[o + 1] << 32)};
+        neumaier(acc_s, acc_c, chunk_terms<YT, WEIGHTED, CHECKED, true, JC, 2>(P, px, B64, A2, o, i0, JC, n_in, oob));
       }
       for (; o < n_out; o++) {
-        const uint64_t A0 = ((uint64_t)S.arel[o * nthr + tid] << 8) + ((uint64_t)S.ahi[o] << 32);
-        neumaier(acc_s, acc_c,
-                 chunk_terms<YT, WEIGHTED, CHECKED, true, JC>(P, px, B64, A0, (int64_t)o * n_in, o, i0, JC, n_in, oob));
+        const uint64_t A1[1] = {((uint64_t)S.arel[o * nthr + tid] << 8) + ((uint64_t)S.ahi[o] << 32)};
+        neumaier(acc_s, acc_c, chunk_terms<YT, WEIGHTED, CHECKED, true, JC, 1>(P, px, B64, A1, o, i0, JC, n_in, oob));
       }
     } else {
       for (int o = 0; o < n_out; o++) {
-        const uint64_t A64 = ((uint64_t)S.arel[o * nthr + tid] << 8) + ((uint64_t)S.ahi[o] << 32);
-        neumaier(acc_s, acc_c, chunk_terms<YT, WEIGHTED, CHECKED, false, JC>(P, px, B64, A64, (int64_t)o * n_in, o,
-                                                                         i0, jn, n_in, oob));
+        const uint64_t A1[1] = {((uint64_t)S.arel[o * nthr + tid] << 8) + ((uint64_t)S.ahi[o] << 32)};
+        neumaier(acc_s, acc_c, chunk_terms<YT, WEIGHTED, CHECKED, false, JC, 1>(P, px, B64, A1, o, i0, jn, n_in, oob));
       }
     }
   }
@@ -619,12 +634,9 @@ __device__ __forceinline__ void tab_gather_body(const FastParams &P, const Pixel
 #pragma unroll
     for (int j = 0; j < JC; j++) B64[j] = (j < jn) ? (uint64_t)__ldg(TB + (int64_t)(i0 + j) * P.No + n) : 0;
     for (int o = 0; o < n_out; o++) {
-      const uint64_t A64 = (uint64_t)__ldg(TA + (int64_t)o * P.No + n);
-      float part = (jn == JC)
-                       ? chunk_terms<YT, WEIGHTED, CHECKED, true, JC>(P, px, B64, A64, (int64_t)o * n_in, o, i0,
-                                                                      JC, n_in, oob)
-                       : chunk_terms<YT, WEIGHTED, CHECKED, false, JC>(P, px, B64, A64, (int64_t)o * n_in, o,
-                                                                       i0, jn, n_in, oob);
+      const uint64_t A1[1] = {(uint64_t)__ldg(TA + (int64_t)o * P.No + n)};
+      float part = (jn == JC) ? chunk_terms<YT, WEIGHTED, CHECKED, true, JC, 1>(P, px, B64, A1, o, i0, JC, n_in, oob)
+                              : chunk_terms<YT, WEIGHTED, CHECKED, false, JC, 1>(P, px, B64, A1, o, i0, jn, n_in, oob);
       neumaier(acc_s, acc_c, part);
     }
   }
@@ -712,18 +724,41 @@ __global__ void __launch_bounds__(256) tab_colowner_kernel(const FastParams P, c
     const uint64_t A64 = (uint64_t)__ldg(TA + (int64_t)o * P.No + n);
     const float xn = ADJ ? __ldg(X + n) : 0.0f;
     const float gn = WG ? __ldg(G + n) : 0.0f;
+    // all leg-table loads first, then the indices; the exact path (a call) only
+    // for points whose terms fall in the ambiguity band
+    uint64_t sj[16];
 #pragma unroll
-    for (int j = 0; j < 16; j++) {
-      if (j < jn) {
-        const int i = i0 + j;
-        const int64_t colk = ((int64_t)o * n_in + i) * P.K;
-        const uint64_t s = A64 + (uint64_t)__ldg(TB + (int64_t)i * P.No + n);
-        const int k = tab_index(P, n, s, colk, o, i);
-        if (k >= 0) {
-          if (ADJ) atomicAdd(hist + (int64_t)j * P.K + k, wc[j] * xn);
-          if (WG) wsum[j] = fmaf(gn, __ldg(Yf + colk + k), wsum[j]);
-        }
+    for (int j = 0; j < 16; j++)
+      sj[j] = (j < jn) ? A64 + (uint64_t)__ldg(TB + (int64_t)(i0 + j) * P.No + n) : 0;
+    uint32_t minlo = 0xffffffffu;
+#pragma unroll
+    for (int j = 0; j < 16; j++)
+      if (j < jn) minlo = min(minlo, (uint32_t)sj[j]);
+    int kj[16];
+    if (minlo >= AMB_LO) {
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        const int64_t colk = ((int64_t)o * n_in + i0 + j) * P.K;
+        const int32_t kk = (int32_t)((uint32_t)(sj[j] >> 32) - (uint32_t)colk);
+        kj[j] = (j >= jn) ? -1 : ((kk >= 0 && kk < P.K) ? kk : (kk == -1 ? 0 : -1));
       }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 16; j++)
+        kj[j] = (j < jn) ? tab_index(P, n, sj[j], ((int64_t)o * n_in + i0 + j) * P.K, o, i0 + j) : -1;
+    }
+    if (WG) {
+      float yv[16];
+#pragma unroll
+      for (int j = 0; j < 16; j++)
+        yv[j] = (kj[j] >= 0) ? __ldg(Yf + ((int64_t)o * n_in + i0 + j) * P.K + kj[j]) : 0.0f;
+#pragma unroll
+      for (int j = 0; j < 16; j++) wsum[j] = fmaf(gn, yv[j], wsum[j]);
+    }
+    if (ADJ) {
+#pragma unroll
+      for (int j = 0; j < 16; j++)
+        if (kj[j] >= 0) atomicAdd(hist + (int64_t)j * P.K + kj[j], wc[j] * xn);
     }
   }
   if (ADJ) {
