@@ -226,6 +226,19 @@ def cg_bench(dev, iters: int = 30, reps: int = 3):
         b.record()
         torch.cuda.synchronize()
         ms.append(a.elapsed_time(b))
+    # the same solve captured in a CUDA graph (no per-launch host overhead)
+    from dream_b200.autograd import CGGraph
+    cgg = CGGraph(op, Y, w, lam=1e-3, iters=iters)
+    cgg.replay()
+    torch.cuda.synchronize()
+    ms_graph = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        cgg.replay()
+        b.record()
+        torch.cuda.synchronize()
+        ms_graph.append(a.elapsed_time(b))
     # per-operator timings (gather / scatter) on the same configuration
     def timed(fn, n=10):
         fn()
@@ -242,7 +255,8 @@ def cg_bench(dev, iters: int = 30, reps: int = 3):
     sums = op.No * op.ncol
     corr = float(torch.dot(x, xt) / (x.norm() * xt.norm()))
     return {"config": "TFM 32x32, K=2048, 256x256 image, lam=1e-3, FP32", "iterations": iters,
-            "cg_ms": min(ms), "residual_reduction": float(res[-1] / res[0]), "corr_with_truth": corr,
+            "cg_ms": min(ms_graph), "cg_eager_ms": min(ms), "residual_reduction": float(res[-1] / res[0]),
+            "corr_with_truth": corr,
             "gather_ms": t_g, "scatter_ms": t_s, "gather_gsum_s": sums / t_g / 1e6,
             "scatter_gsum_s": sums / t_s / 1e6}
 

@@ -202,3 +202,31 @@ def cg_reconstruct(op: DASOperator, Y, w, lam: float = 1e-3, iters: int = 30, x0
         p = r + (rs_new / rs) * p
         rs = rs_new
     return x, torch.stack(hist).sqrt() if hist else torch.zeros(0, device=b.device)
+
+
+class CGGraph:
+    """``cg_reconstruct`` captured once in a CUDA graph.
+
+    ``Y`` and ``w`` are copied into static buffers (``self.Y``, ``self.w``);
+    write new A-scans or weights into them and call ``replay()`` to solve
+    again without any host-side launch overhead. ``self.x`` and
+    ``self.residuals`` hold the latest solution.
+    """
+
+    def __init__(self, op: DASOperator, Y, w, lam: float = 1e-3, iters: int = 30):
+        self.op = op
+        self.Y = op._ascans(Y).clone()
+        self.w = w.to(device=op.device, dtype=torch.float32).clone()
+        side = torch.cuda.Stream(op.device)
+        side.wait_stream(torch.cuda.current_stream(op.device))
+        with torch.cuda.stream(side):
+            cg_reconstruct(op, self.Y, self.w, lam, 2)  # warm-up outside the capture
+        torch.cuda.current_stream(op.device).wait_stream(side)
+        torch.cuda.synchronize(op.device)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.x, self.residuals = cg_reconstruct(op, self.Y, self.w, lam, iters)
+
+    def replay(self):
+        self.graph.replay()
+        return self.x, self.residuals

@@ -155,10 +155,14 @@ def das_generic(dtype, Y, Gt, Gr, Ro, dt, delay, cp, method, err_level="stop", d
 
 
 def _torch_fortran(t, dtype, device):
+    """Column-major device copy. Host data in pinned memory is uploaded
+    asynchronously (the caller's stream orders it before the kernel)."""
     import torch
     tdt = torch.float64 if np.dtype(dtype) == np.float64 else torch.float32
     if not _is_torch(t):
         t = torch.as_tensor(np.asarray(t))
+    if t.device.type == "cpu" and t.dtype == tdt:
+        t = t.to(device=device, non_blocking=t.is_pinned())
     t = t.to(device=device, dtype=tdt)
     if t.dim() == 0:
         t = t.reshape(1, 1)
@@ -264,18 +268,28 @@ _STORAGE = {"f32": _lib.PREC_F32_STORE, "bf16": _lib.PREC_BF16_STORE}
 def grid_hint(Ro) -> int:
     """Number of leading image points that share x and y (the fastest grid
     axis, e.g. Nz for ``meshgrid(x, z)`` flattened column-major), or 0 when
-    it does not divide the number of points."""
+    it does not divide the number of points. Only speed depends on it, so
+    the scan stops at the first change (growing windows of points)."""
     No = int(Ro.shape[0])
     if No == 0:
         return 0
-    if _is_torch(Ro):
-        import torch
-        ch = torch.nonzero((Ro[:, 0] != Ro[0, 0]) | (Ro[:, 1] != Ro[0, 1]))
-        n = int(ch[0, 0].item()) if ch.numel() else No
-    else:
-        R = np.asarray(Ro)
-        ch = np.nonzero((R[:, 0] != R[0, 0]) | (R[:, 1] != R[0, 1]))[0]
-        n = int(ch[0]) if ch.size else No
+    n, lo, win = No, 1, 1024
+    while lo < No:
+        hi = min(No, lo + win)
+        blk = Ro[lo:hi]
+        if _is_torch(Ro):
+            import torch
+            ch = torch.nonzero((blk[:, 0] != Ro[0, 0]) | (blk[:, 1] != Ro[0, 1]))
+            if ch.numel():
+                n = lo + int(ch[0, 0].item())
+                break
+        else:
+            R = np.asarray(blk)
+            ch = np.nonzero((R[:, 0] != Ro[0, 0]) | (R[:, 1] != Ro[0, 1]))[0]
+            if ch.size:
+                n = lo + int(ch[0])
+                break
+        lo, win = hi, win * 4
     return n if (n > 0 and No % n == 0 and n < No) else 0
 
 

@@ -10,6 +10,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 namespace dream {
 
 enum Method : int { SAFT = 0, TFM = 1, RCA_COLTX = 2, RCA_ROWTX = 3 };
@@ -59,6 +63,25 @@ __device__ __forceinline__ int trunc_index(float p) {
 __device__ __forceinline__ void add_count(unsigned long long *ctr, unsigned int v) {
   unsigned int s = __reduce_add_sync(0xffffffffu, v);
   if (ctr != nullptr && (threadIdx.x & 31) == 0 && s) atomicAdd(ctr, (unsigned long long)s);
+}
+
+// Raises a kernel's dynamic shared-memory limit once per (kernel, device):
+// later launches (including ones being captured into a CUDA graph) then issue
+// no attribute call.
+template <class F>
+inline cudaError_t ensure_smem(F *kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, size_t> done;
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  auto key = std::make_pair(reinterpret_cast<const void *>(kernel), dev);
+  auto it = done.find(key);
+  if (it != done.end() && it->second >= bytes) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) done[key] = bytes;
+  return e;
 }
 
 }  // namespace dream

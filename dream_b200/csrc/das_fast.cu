@@ -513,7 +513,7 @@ static cudaError_t launch_fast_t(const FastParams &P, cudaStream_t st) {
   const int nthr = P.tile_f * P.tile_s;
   const size_t smem = fast_smem_bytes(P, nthr);
   auto kern = (P.jc == 8) ? das_fast_kernel<YT, W, 8> : das_fast_kernel<YT, W, 16>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = ensure_smem(kern, smem);
   if (e != cudaSuccess) return e;
   const int64_t gx = (P.n_fast + P.tile_f - 1) / P.tile_f;
   const int64_t gy = P.slow_tile1 - P.slow_tile0;
@@ -837,13 +837,13 @@ cudaError_t launch_tab_colowner(const FastParams &P, const int64_t *TA, const in
   dim3 grid((unsigned)n_out, (unsigned)groups, (unsigned)splits);
   cudaError_t e;
   if (adj && wg) {
-    e = cudaFuncSetAttribute(tab_colowner_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = ensure_smem(tab_colowner_kernel<true, true>, smem);
     if (e == cudaSuccess) tab_colowner_kernel<true, true><<<grid, 256, smem, st>>>(P, TA, TB, X, G, Ya, dW, cw, splits);
   } else if (adj) {
-    e = cudaFuncSetAttribute(tab_colowner_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = ensure_smem(tab_colowner_kernel<true, false>, smem);
     if (e == cudaSuccess) tab_colowner_kernel<true, false><<<grid, 256, smem, st>>>(P, TA, TB, X, G, Ya, dW, cw, splits);
   } else {
-    e = cudaFuncSetAttribute(tab_colowner_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = ensure_smem(tab_colowner_kernel<false, true>, smem);
     if (e == cudaSuccess) tab_colowner_kernel<false, true><<<grid, 256, smem, st>>>(P, TA, TB, X, G, Ya, dW, cw, splits);
   }
   if (e != cudaSuccess) return e;

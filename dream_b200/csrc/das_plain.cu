@@ -250,10 +250,8 @@ template <class T, int M, bool UNI, bool TAB>
 static cudaError_t launch_one(const PlainParams<T> &P, int bd, size_t smem, cudaStream_t st) {
   auto kern = (sizeof(T) == 4 && P.bigk) ? das_plain_kernel<T, M, UNI, TAB, true>
                                          : das_plain_kernel<T, M, UNI, TAB, false>;
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-  }
+  cudaError_t e = ensure_smem(kern, smem);
+  if (e != cudaSuccess) return e;
   int64_t grid = (P.no1 - P.no0 + bd - 1) / bd;
   kern<<<(unsigned)grid, bd, smem, st>>>(P);
   return cudaGetLastError();
