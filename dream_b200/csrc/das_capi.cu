@@ -107,6 +107,9 @@ struct dream_das_plan {
   int64_t n_fast = 0;          // grid hint (0: none)
   int tile_f = 0, tile_s = 0;  // user / autotuner tile (0: automatic)
   int jc = 0;                  // user / autotuner inner chunk (0: automatic)
+  // host-pointer runs of FP32/BF16-storage plans: A-scan upload stream
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t chunk_ev[8] = {nullptr};
   // geometry-bound operator
   bool bound = false;
   FastParams geo{};
@@ -294,7 +297,7 @@ void fast_tile(const dream_das_plan *p, int n_out, int &tf, int &ts, int &wf) {
 
 int launch_fast_plan(dream_das_plan *p, const void *dY, const void *dRo, const void *dGt, const void *dGr,
                      double dt, int delay_type, const void *ddelay, double cp, const float *dW, float *dIm,
-                     unsigned long long *doob, cudaStream_t st) {
+                     unsigned long long *doob, cudaStream_t st, int in_lo = 0, int in_hi = 0, int accumulate = 0) {
   if (delay_type != DREAM_DELAY_SINGLE && delay_type != DREAM_DELAY_MULTIPLE)
     return fail(DREAM_ERR_ARGUMENT, "unknown delay type");
   if (ddelay == nullptr) return fail(DREAM_ERR_ARGUMENT, "delay pointer is NULL");
@@ -327,6 +330,9 @@ int launch_fast_plan(dream_das_plan *p, const void *dY, const void *dRo, const v
   F.w = dW;
   F.Im = dIm;
   F.oob = doob;
+  F.in_lo = in_lo;
+  F.in_hi = in_hi;
+  F.accumulate = accumulate;
   const bool bf16 = p->precision == DREAM_PREC_BF16_STORE;
   const int64_t tpp = std::max<int64_t>(terms_per_pixel(p), 1);
   if (method == DREAM_DAS_SAFT) {
@@ -439,6 +445,9 @@ void dream_das_plan_destroy(dream_das_plan *p) {
     p->bTB.release();
     p->bRange.release();
     if (p->h_oob) cudaFreeHost(p->h_oob);
+    for (auto &ev : p->chunk_ev)
+      if (ev) cudaEventDestroy(ev);
+    if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
     if (p->stream) cudaStreamDestroy(p->stream);
   }
   delete p;
@@ -868,11 +877,59 @@ int dream_das_run(dream_das_plan *p, const void *Y, const void *Ro, const void *
   if ((r = p->bGr.ensure((size_t)nr * 3 * gs))) return r;
   if ((r = p->bDelay.ensure((size_t)(multi ? p->No : 1) * gs))) return r;
   if ((r = p->bIm.ensure((size_t)p->No * is))) return r;
-  if (ny > 0) CU(cudaMemcpyAsync(p->bY.p, Y, (size_t)ny * ys, cudaMemcpyHostToDevice, st));
+  // FP32/BF16-storage TFM and RCA: the A-scans are uploaded in chunks of
+  // inner elements on a copy stream while the kernel beamforms the chunks
+  // already resident, adding each chunk's terms into the image.
+  const bool pipelined = is_fast(p) && method != DREAM_DAS_SAFT && p->No > 0 && p->K > 0 &&
+                         (size_t)ny * 4 >= (size_t(8) << 20);
+  if (ny > 0 && !pipelined) CU(cudaMemcpyAsync(p->bY.p, Y, (size_t)ny * ys, cudaMemcpyHostToDevice, st));
   if (p->No > 0) CU(cudaMemcpyAsync(p->bRo.p, Ro, (size_t)p->No * 3 * gs, cudaMemcpyHostToDevice, st));
   if (p->Nt > 0) CU(cudaMemcpyAsync(p->bGt.p, Gt, (size_t)p->Nt * 3 * gs, cudaMemcpyHostToDevice, st));
   if (nr > 0) CU(cudaMemcpyAsync(p->bGr.p, Gr, (size_t)nr * 3 * gs, cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync(p->bDelay.p, delay, (size_t)(multi ? p->No : 1) * gs, cudaMemcpyHostToDevice, st));
+  if (pipelined) {
+    const int n_out = (method == DREAM_DAS_RCA_ROWTX) ? (int)p->Nr : (int)p->Nt;
+    const int n_in = (method == DREAM_DAS_RCA_ROWTX) ? (int)p->Nt : (int)p->Nr;
+    const bool bf16 = p->precision == DREAM_PREC_BF16_STORE;
+    if (bf16 && (r = p->bY16.ensure((size_t)ny * 2))) return r;
+    if (p->copy_stream == nullptr) CU(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+    for (auto &ev : p->chunk_ev)
+      if (ev == nullptr) CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    int check = 0;
+    if (method >= DREAM_DAS_RCA_COLTX && (check = check_rca_edges(p->Nt, p->Nr))) return check;
+    // chunk boundaries on multiples of 16 inner elements (the register chunk)
+    const int nch = std::max(1, std::min(4, (n_in + 15) / 16));
+    unsigned long long *doob = (unsigned long long *)p->bOob.p;
+    CU(cudaMemsetAsync(doob, 0, sizeof(unsigned long long), st));
+    // the copy stream must not overwrite A-scans a previous call still reads
+    CU(cudaEventRecord(p->chunk_ev[7], st));
+    CU(cudaStreamWaitEvent(p->copy_stream, p->chunk_ev[7], 0));
+    const size_t pitch = (size_t)n_in * p->K * 4;
+    for (int c = 0; c < nch; c++) {
+      const int lo = std::min(n_in, ((c * n_in / nch) + 15) / 16 * 16);
+      const int hi = (c == nch - 1) ? n_in : std::min(n_in, (((c + 1) * n_in / nch) + 15) / 16 * 16);
+      if (hi <= lo) continue;
+      const size_t off = (size_t)lo * p->K * 4, width = (size_t)(hi - lo) * p->K * 4;
+      CU(cudaMemcpy2DAsync((char *)p->bY.p + off, pitch, (const char *)Y + off, pitch, width, (size_t)n_out,
+                           cudaMemcpyHostToDevice, p->copy_stream));
+      if (bf16) {
+        CU(convert_f32_to_bf16_2d((const float *)p->bY.p + (size_t)lo * p->K, (uint16_t *)p->bY16.p + (size_t)lo * p->K,
+                                  n_out, (int64_t)(hi - lo) * p->K, (int64_t)n_in * p->K, p->copy_stream));
+        p->launches++;
+      }
+      CU(cudaEventRecord(p->chunk_ev[c], p->copy_stream));
+      CU(cudaStreamWaitEvent(st, p->chunk_ev[c], 0));
+      r = launch_fast_plan(p, bf16 ? p->bY16.p : p->bY.p, p->bRo.p, p->bGt.p, p->bGr.p, dt, delay_type, p->bDelay.p,
+                           cp, nullptr, (float *)p->bIm.p, doob, st, lo, hi, c > 0 ? 1 : 0);
+      if (r) return r;
+    }
+    CU(cudaMemcpyAsync(Im, p->bIm.p, (size_t)p->No * is, cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(p->h_oob, doob, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    uint64_t oob = *p->h_oob;
+    if (oob_count) *oob_count = (int64_t)oob;
+    return status_from_oob(oob, err_level);
+  }
   const void *dYrun = p->bY.p;
   if (p->precision == DREAM_PREC_BF16_STORE && ny > 0) {
     if ((r = p->bY16.ensure((size_t)ny * 2))) return r;

@@ -259,11 +259,11 @@ __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &p
 
 template <class YT, bool WEIGHTED, bool CHECKED, int JC>
 __device__ __forceinline__ void tile_loop(const FastParams &P, const Pixel &px, const TileShared &S, int tid,
-                                          int nthr, int n_out, int n_in, float &acc_s, float &acc_c,
-                                          unsigned int &oob) {
+                                          int nthr, int n_out, int n_in, int i_lo, int i_hi, float &acc_s,
+                                          float &acc_c, unsigned int &oob) {
   const int64_t K = P.K;
-  for (int i0 = 0; i0 < n_in; i0 += JC) {
-    const int jn = min(JC, n_in - i0);
+  for (int i0 = i_lo; i0 < i_hi; i0 += JC) {
+    const int jn = min(JC, i_hi - i0);
     uint64_t B64[JC];
 #pragma unroll
     for (int j = 0; j < JC; j++) {
@@ -312,6 +312,8 @@ __device__ __forceinline__ void fast_tile(const FastParams &P, int64_t tfi, int6
   const int lane = tid & 31, warp = tid >> 5;
   const int n_out = (P.method == RCA_ROWTX) ? P.Nr : P.Nt;
   const int n_in = (P.method == RCA_ROWTX) ? P.Nt : P.Nr;
+  // inner elements of this launch: all of them unless the caller sets a range
+  const int i_lo = P.in_lo, i_hi = P.in_hi > 0 ? P.in_hi : n_in;
 
   TileShared S;
   S.minA = reinterpret_cast<int *>(smem_raw);
@@ -359,7 +361,7 @@ __device__ __forceinline__ void fast_tile(const FastParams &P, int64_t tfi, int6
       atomicMax(&S.maxA[o], mx);
     }
   }
-  for (int i = 0; i < n_in; i++) {
+  for (int i = i_lo; i < i_hi; i++) {
     int fl;
     bool ok;
     fix24(A_mul_Fs(P, inner_leg(P, px, i)), fl, ok);
@@ -380,7 +382,7 @@ __device__ __forceinline__ void fast_tile(const FastParams &P, int64_t tfi, int6
     loA = min(loA, S.minA[o]);
     hiA = max(hiA, S.maxA[o]);
   }
-  for (int i = 0; i < n_in; i++) {
+  for (int i = i_lo; i < i_hi; i++) {
     ext = max(ext, S.maxB[i] - S.minB[i]);
     loB = min(loB, S.minB[i]);
     hiB = max(hiB, S.maxB[i]);
@@ -398,7 +400,7 @@ __device__ __forceinline__ void fast_tile(const FastParams &P, int64_t tfi, int6
     // every term through the exact FP64 index
     for (int o = 0; o < n_out; o++) {
       float part = 0.0f;
-      for (int i = 0; i < n_in; i++) {
+      for (int i = i_lo; i < i_hi; i++) {
         int k;
         const int64_t col = (int64_t)o * n_in + i;
         if (exact_index(P, px, o, i, k)) {
@@ -416,10 +418,12 @@ __device__ __forceinline__ void fast_tile(const FastParams &P, int64_t tfi, int6
       S.arel[o * nthr + tid] = S.arel[o * nthr + tid] - ((uint32_t)S.minA[o] << FB) + DELTA_UNITS;
     for (int o = tid; o < n_out; o += nthr) S.ahi[o] = (uint32_t)((int64_t)o * n_in * P.K + S.minA[o]);
     __syncthreads();
-    if (in_bounds) tile_loop<YT, WEIGHTED, false, JC>(P, px, S, tid, nthr, n_out, n_in, acc_s, acc_c, oob);
-    else tile_loop<YT, WEIGHTED, true, JC>(P, px, S, tid, nthr, n_out, n_in, acc_s, acc_c, oob);
+    if (in_bounds)
+      tile_loop<YT, WEIGHTED, false, JC>(P, px, S, tid, nthr, n_out, n_in, i_lo, i_hi, acc_s, acc_c, oob);
+    else
+      tile_loop<YT, WEIGHTED, true, JC>(P, px, S, tid, nthr, n_out, n_in, i_lo, i_hi, acc_s, acc_c, oob);
   }
-  if (active) P.Im[no] = acc_s + acc_c;
+  if (active) P.Im[no] = P.accumulate ? P.Im[no] + (acc_s + acc_c) : acc_s + acc_c;
   add_count(P.oob, active ? oob : 0u);
 }
 
@@ -555,6 +559,24 @@ int batch_prepare(size_t smem, bool bf16) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, das_batch_kernel<float>, 128, smem);
   }
   return n;
+}
+
+__global__ void f32_to_bf16_2d_kernel(const float *__restrict__ x, __nv_bfloat16 *__restrict__ y, int64_t rows,
+                                      int64_t row_elems, int64_t pitch) {
+  const int64_t n = rows * row_elems;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = q / row_elems, e = q - r * row_elems;
+    y[r * pitch + e] = __float2bfloat16_rn(x[r * pitch + e]);
+  }
+}
+
+cudaError_t convert_f32_to_bf16_2d(const float *x, void *y, int64_t rows, int64_t row_elems, int64_t pitch,
+                                   cudaStream_t st) {
+  const int64_t n = rows * row_elems;
+  if (n <= 0) return cudaSuccess;
+  int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
+  f32_to_bf16_2d_kernel<<<blocks, 256, 0, st>>>(x, reinterpret_cast<__nv_bfloat16 *>(y), rows, row_elems, pitch);
+  return cudaGetLastError();
 }
 
 cudaError_t convert_f32_to_bf16(const float *x, void *y, int64_t n, cudaStream_t st) {

@@ -28,11 +28,18 @@ struct FastParams {
   int jc;                  // inner elements per register chunk: 8 or 16
   int64_t slow_tile0, slow_tile1;  // slow-tile range of this launch
   int64_t no0, no1;                // point range (SAFT launches)
+  // inner-element range [in_lo, in_hi) of this launch (in_hi == 0: all inner
+  // elements) and whether to add into Im instead of writing it
+  int in_lo, in_hi;
+  int accumulate;
 };
 
 size_t fast_smem_bytes(const FastParams &P, int nthr);
 cudaError_t launch_fast(const FastParams &P, bool bf16, cudaStream_t st);
 cudaError_t convert_f32_to_bf16(const float *x, void *y, int64_t n, cudaStream_t st);
+// rows x row_elems block of a row-pitched array (same offsets in x and y)
+cudaError_t convert_f32_to_bf16_2d(const float *x, void *y, int64_t rows, int64_t row_elems, int64_t pitch,
+                                   cudaStream_t st);
 
 // Geometry-bound operator (leg tables; FP32 samples).
 // range: 7 ints of device scratch written by build_leg_tables.

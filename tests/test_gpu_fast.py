@@ -203,3 +203,39 @@ def test_rca_full_config_bf16():
     ref = oracle.das(sub.Y, sub.Gt, sub.Gr, sub.Ro, sub.dt, sub.delay, sub.cp, s.method, "ignore")[0]
     scale = max(np.abs(Im).max(), np.abs(ref).max())
     assert np.abs(Im[sel] - ref).max() <= 1e-3 * scale
+
+
+@pytest.mark.parametrize("storage", ["f32", "bf16"])
+@pytest.mark.parametrize("spec", [
+    dict(kind="tfm", kw=dict(seed=71, n_el=40, K=1800, nx=48, nz=40)),
+    dict(kind="rca", kw=dict(seed=72, n_cols=32, n_rows=32, K=2600, nx=6, ny=6, nz=10, method="rca_rowtx")),
+    dict(kind="rca", kw=dict(seed=73, n_cols=32, n_rows=32, K=2600, nx=6, ny=6, nz=10, method="rca_coltx")),
+], ids=["tfm", "rca_rowtx", "rca_coltx"])
+def test_pipelined_host_upload_matches_device_path(spec, storage):
+    """Host arrays (>= 8 MB of A-scans) through the C ABI's host entry
+    (dream_das_run), which uploads them in chunks that overlap the
+    beamforming; the image equals the device-pointer path's up to the order in
+    which the chunks' partial images are added."""
+    import ctypes
+    from dream_b200 import _lib
+    from dream_b200.beamformer import _fast_plan, das_mixed, grid_hint, parse_method
+    s = build_scene(spec)
+    assert s.Y.nbytes // 2 >= 8 << 20
+    Y = np.asfortranarray(s.Y.astype(np.float32))
+    f = lambda a: np.asfortranarray(np.asarray(a, dtype=np.float64))
+    Gt, Gr, Ro, dl = f(s.Gt), f(s.Gr), f(s.Ro), f(s.delay)
+    m = parse_method(s.method)
+    prec = _lib.PREC_F32_STORE if storage == "f32" else _lib.PREC_BF16_STORE
+    plan = _fast_plan(m, Y.shape[0], Ro.shape[0], Gt.shape[0], Gr.shape[0], prec, 0, grid_hint(Ro))
+    host = np.zeros(Ro.shape[0], dtype=np.float32)
+    ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    st = _lib.load().dream_das_run(plan.handle, ptr(Y), ptr(Ro), ptr(Gt), ptr(Gr), s.dt, _lib.DELAY_SINGLE,
+                                   ptr(dl), s.cp, ptr(host), _lib.LVL_IGNORE, None)
+    assert st >= 0, _lib.last_error()
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=np.float64).T)).cuda().t()
+    Yd = torch.from_numpy(np.ascontiguousarray(s.Y.astype(np.float32).T)).cuda().t()
+    dev = das_mixed(Yd, t(s.Gt), t(s.Gr), t(s.Ro), s.dt, t(s.delay), s.cp, s.method, "ignore", "cuda",
+                    storage).cpu().numpy()
+    assert np.abs(host - dev).max() <= 2e-6 * np.abs(dev).max()
+    ref, _, _ = oracle_on_stored(s, storage)
+    assert np.abs(host - ref).max() <= 2e-6 * np.abs(ref).max()
