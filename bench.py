@@ -189,6 +189,46 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def measure_peaks(dev):
+    """Project-written microbenchmarks (dream_b200/peaks/peaks.cu): the L2
+    gather rates the DAS gathers are bounded by, and the FP32/FP64/integer
+    pipe rates, measured on this GPU."""
+    import torch
+    L = ctypes.CDLL(os.path.join(ROOT, "dream_b200", "libdream_peaks.so"))
+    L.dream_peaks_run.restype = ctypes.c_double
+    L.dream_peaks_run.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+    log2w = 23  # 32 MiB of floats: L2-resident
+    buf = torch.randn(1 << log2w, device=dev)
+    blocks, threads = 148 * 8, 256
+    sink = torch.zeros(blocks * threads, device=dev)
+    ops = ctypes.c_double(0.0)
+
+    def run(kind, iters):
+        L.dream_peaks_run(kind, ctypes.c_void_p(buf.data_ptr()), log2w, blocks, threads, 8,
+                          ctypes.c_void_p(sink.data_ptr()), ctypes.byref(ops))  # warm-up
+        best = None
+        for _ in range(3):
+            ms = L.dream_peaks_run(kind, ctypes.c_void_p(buf.data_ptr()), log2w, blocks, threads, iters,
+                                   ctypes.c_void_p(sink.data_ptr()), ctypes.byref(ops))
+            if ms > 0:
+                best = ms if best is None else min(best, ms)
+        return ops.value / (best * 1e-3) if best else None
+
+    sec = run(0, 512)
+    das = run(1, 512)
+    f32 = run(2, 4096)
+    f64 = run(3, 1024)
+    i32 = run(4, 2048)
+    return {"l2_random_sector_GBps": sec * 32 / 1e9 if sec else None,
+            "l2_random_sector_loads_per_s": sec,
+            "l2_das_gather_words_per_s": das, "l2_das_gather_GBps": das * 4 / 1e9 if das else None,
+            "fp32_tflops": f32 * 2 / 1e12 if f32 else None, "fp64_tflops": f64 * 2 / 1e12 if f64 else None,
+            "int32_tops": i32 / 1e12 if i32 else None,
+            "how": "dream_b200/peaks/peaks.cu: 1184 CTAs x 256 threads, best of 3, CUDA events; gathers over "
+                   "a 32 MiB L2-resident buffer"}
+
+
 def read_traffic(kernel_key: str):
     """Per-launch DRAM bytes of a kernel from the committed ncu summary."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
@@ -339,9 +379,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--peaks", action="store_true", help="print the measured roofline peaks and exit")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.peaks:
+        import torch
+        print(json.dumps(measure_peaks(torch.device("cuda", 0))))
+        return
 
     import torch
     import torch.distributed as dist
@@ -474,6 +519,7 @@ def main():
     cg = cg_bench(dev)
     batched = batch_bench(dev)
     rca = rca_bench(dev)
+    peaks = measure_peaks(dev)
 
     if world > 1:
         dist.destroy_process_group()
@@ -506,6 +552,12 @@ def main():
         "batched": batched,
         "rca": rca,
         "autotuned": {("bf16_store" if k == _lib.PREC_BF16_STORE else "f32_store"): v for k, v in tuned.items()},
+        "roofline_l2": {"achieved_words_per_s": sums / (step_ms * 1e-3),
+                        "peak_das_gather_words_per_s": peaks["l2_das_gather_words_per_s"],
+                        "frac": (sums / (step_ms * 1e-3)) / peaks["l2_das_gather_words_per_s"]
+                        if peaks["l2_das_gather_words_per_s"] else None,
+                        "note": "gathered samples per second against the measured L2 DAS-shaped gather rate"},
+        "peaks": peaks,
         "gpu_launches": int(launches_h),
         "clocks": clk,
     }

@@ -11,7 +11,9 @@ import os
 import threading
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libdream_das.so")
+# DREAM_DAS_CHECKED=1 selects the bounds-checked build (python -m dream_b200.build --checked)
+CHECKED = os.environ.get("DREAM_DAS_CHECKED", "0") not in ("", "0")
+LIB_PATH = os.path.join(HERE, "libdream_das_checked.so" if CHECKED else "libdream_das.so")
 
 # status codes (mirror include/dream_das.h)
 STATUS_NONE = 0
@@ -47,6 +49,8 @@ SIGNATURES = {
     "dream_das_plan_num_points": (_i64, [_vp]),
     "dream_das_plan_num_ascans": (_i64, [_vp]),
     "dream_das_plan_launch_count": (_i64, [_vp]),
+    "dream_das_checked_build": (ctypes.c_int, []),
+    "dream_das_plan_bound_violations": (_i64, [_vp]),
     "dream_das_uni_run": (_i, [_vp, _vp, _pd, _d, _d, _d, _vp, _i, _pi64]),
     "dream_das_uni_run_device": (_i, [_vp, _vp, _pd, _d, _d, _d, _vp, _i, _pi64, _vp]),
     "dream_das_set_grid_hint": (_i, [_vp, _i64]),
@@ -90,7 +94,8 @@ def load():
         if _lib is None:
             if not os.path.exists(LIB_PATH):
                 raise ImportError(
-                    f"{LIB_PATH} is missing: build it with `python -m dream_b200.build` "
+                    f"{LIB_PATH} is missing: build it with `python -m dream_b200.build"
+                    f"{' --checked' if CHECKED else ''}` "
                     "(the CUDA backend has no CPU fallback)")
             L = ctypes.CDLL(LIB_PATH)
             for name, (res, args) in SIGNATURES.items():

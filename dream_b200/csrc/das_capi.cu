@@ -114,6 +114,7 @@ struct dream_das_plan {
   bool bound = false;
   FastParams geo{};
   DevBuf bTA, bTB, bRange;
+  DevBuf bBad;  // gather index violations (bounds-checked builds only)
   int sm_count = 148;
   unsigned long long *h_oob = nullptr;  // pinned
   std::atomic<bool> cancelled{false};
@@ -204,7 +205,26 @@ int64_t uni_count(double mn, double d, double mx, bool f32) {
   return (int64_t)(int)q;
 }
 
+#ifdef DREAM_DAS_CHECKED
+constexpr bool kChecked = true;
+#else
+constexpr bool kChecked = false;
+#endif
+
+// Device counter of gather indices outside Y (bounds-checked builds; NULL in
+// the normal build, whose kernels never test the index).
+unsigned long long *bad_counter(dream_das_plan *p) {
+  if (!kChecked) return nullptr;
+  if (p->bBad.p == nullptr) {
+    if (p->bBad.ensure(sizeof(unsigned long long))) return nullptr;
+    if (cudaMemset(p->bBad.p, 0, sizeof(unsigned long long)) != cudaSuccess) return nullptr;
+  }
+  return (unsigned long long *)p->bBad.p;
+}
+
 int launch_plain(dream_das_plan *p, PlainLaunch &L, cudaStream_t st) {
+  L.ny = p->K * num_columns(p);
+  L.bad = bad_counter(p);
   // Pixel chunks keep a cancellation request observable between launches.
   const int64_t tpp = std::max<int64_t>(terms_per_pixel(p), 1);
   int64_t chunk = std::max<int64_t>(int64_t(1) << 16, (int64_t(1) << 33) / tpp);
@@ -315,6 +335,8 @@ int launch_fast_plan(dream_das_plan *p, const void *dY, const void *dRo, const v
   memset(&F, 0, sizeof(F));
   F.method = method;
   F.Y = dY;
+  F.ny = p->K * num_columns(p);
+  F.bad = bad_counter(p);
   F.K = p->K;
   F.Ro = (const double *)dRo;
   F.No = p->No;
@@ -466,6 +488,19 @@ int64_t dream_das_plan_num_points(const dream_das_plan *p) { return p ? p->No : 
 int64_t dream_das_plan_num_ascans(const dream_das_plan *p) { return p ? num_columns(p) : -1; }
 
 int64_t dream_das_plan_launch_count(const dream_das_plan *p) { return p ? p->launches.load() : -1; }
+
+int dream_das_checked_build(void) { return kChecked ? 1 : 0; }
+
+int64_t dream_das_plan_bound_violations(dream_das_plan *p) {
+  if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
+  if (!kChecked || p->bBad.p == nullptr) return 0;
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  unsigned long long v = 0;
+  CU(cudaDeviceSynchronize());
+  CU(cudaMemcpy(&v, p->bBad.p, sizeof(v), cudaMemcpyDeviceToHost));
+  return (int64_t)v;
+}
 
 int dream_das_set_grid_hint(dream_das_plan *p, int64_t n_fast) {
   if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");

@@ -58,6 +58,21 @@ __device__ __forceinline__ int trunc_index(float p) {
   return __float_as_int(v) - 0x4B000000;
 }
 
+// Bounds-checked builds (nvcc -DDREAM_DAS_CHECKED, `python -m dream_b200.build
+// --checked`): every A-scan gather verifies its element index against the
+// buffer's extent; a violation is counted in *bad and the load is skipped.
+// The normal build compiles this to the plain load.
+template <class T>
+__device__ __forceinline__ bool gather_ok(int64_t i, int64_t n, unsigned long long *bad) {
+#ifdef DREAM_DAS_CHECKED
+  if (i < 0 || i >= n) {
+    if (bad) atomicAdd(bad, 1ull);
+    return false;
+  }
+#endif
+  return true;
+}
+
 // Warp-aggregated add of a per-thread count to a global counter. Must be
 // called by all 32 lanes of the warp.
 __device__ __forceinline__ void add_count(unsigned long long *ctr, unsigned int v) {

@@ -74,6 +74,11 @@ struct Pixel {
 
 __device__ __forceinline__ double A_mul_Fs(const FastParams &P, double leg) { return Ar<double>::mul(leg, P.Fs); }
 
+// Elements in Y: K times the A-scan columns (Nt for SAFT, Nt*Nr otherwise).
+__device__ __forceinline__ int64_t y_count(const FastParams &P) {
+  return P.ny ? P.ny : P.K * (int64_t)P.Nt * (P.method == SAFT ? 1 : P.Nr);
+}
+
 __device__ __forceinline__ void pixel_of(const FastParams &P, int64_t no, Pixel &px) {
   using A = Ar<double>;
   px.xo = P.Ro[no];
@@ -165,7 +170,7 @@ __device__ __noinline__ float exact_partial(const FastParams &P, const Pixel &px
     int k;
     const int64_t col = (int64_t)o * n_in + i0 + j;
     if (exact_index(P, px, o, i0 + j, k)) {
-      float y = load_sample(Y + col * P.K + k);
+      const float y = gather_ok<float>(col * P.K + k, y_count(P), P.bad) ? load_sample(Y + col * P.K + k) : 0.0f;
       part = WEIGHTED ? fmaf(__ldg(P.w + col), y, part) : part + y;
     } else {
       oob++;
@@ -208,11 +213,15 @@ __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &p
           // anything else is out of bounds.
           const int64_t col0 = ((int64_t)(o0 + q) * n_in + i0 + j) * K;
           const int32_t kk = (int32_t)(off - (uint32_t)col0);  // floor index, exact modulo 2^32
-          if (kk >= 0 && kk < K) y[q][j] = load_sample(Y + col0 + kk);
-          else if (kk == -1) y[q][j] = load_sample(Y + col0);
-          else oob_chunk[q]++;
+          if (kk >= 0 && kk < K) {
+            if (gather_ok<float>(col0 + kk, y_count(P), P.bad)) y[q][j] = load_sample(Y + col0 + kk);
+          } else if (kk == -1) {
+            y[q][j] = load_sample(Y + col0);
+          } else {
+            oob_chunk[q]++;
+          }
         } else {
-          y[q][j] = load_sample(elem_addr(Y, off));
+          if (gather_ok<float>((int64_t)off, y_count(P), P.bad)) y[q][j] = load_sample(elem_addr(Y, off));
         }
       }
     }
@@ -476,7 +485,8 @@ __global__ void __launch_bounds__(256) das_fast_saft_kernel(const FastParams P) 
                         P.ocp);
     double p = A::mul(A::mul(2.0, A::add(l, px.delay_ms)), P.Fs);
     if (P.K > 0 && p > -1.0 && p < (double)P.K) {
-      float y = load_sample(Y + (int64_t)n * P.K + trunc_index(p));
+      const int64_t gi = (int64_t)n * P.K + trunc_index(p);
+      float y = gather_ok<float>(gi, y_count(P), P.bad) ? load_sample(Y + gi) : 0.0f;
       part = WEIGHTED ? fmaf(__ldg(P.w + n), y, part) : part + y;
     } else {
       oob++;

@@ -32,6 +32,8 @@ struct FastParams {
   // elements) and whether to add into Im instead of writing it
   int in_lo, in_hi;
   int accumulate;
+  int64_t ny;               // elements in Y (bounds-checked builds; 0: K * columns)
+  unsigned long long *bad;  // gather index violations (bounds-checked builds)
 };
 
 size_t fast_smem_bytes(const FastParams &P, int nthr);

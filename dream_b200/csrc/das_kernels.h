@@ -39,6 +39,8 @@ struct PlainLaunch {
   int64_t Nx, Ny, Nz;
   void *Im;
   unsigned long long *oob;
+  int64_t ny;               // elements in Y
+  unsigned long long *bad;  // gather index violations (bounds-checked builds)
 };
 
 cudaError_t launch_plain_f64(const PlainLaunch &L, cudaStream_t st);

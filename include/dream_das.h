@@ -171,6 +171,22 @@ int dream_das_uni_run_device(dream_das_plan *plan, const void *dY, const double 
 int64_t dream_das_plan_launch_count(const dream_das_plan *plan);
 
 /*
+ * 1 when this library is the bounds-checked build (nvcc -DDREAM_DAS_CHECKED,
+ * libdream_das_checked.so), 0 otherwise. In that build every A-scan gather of
+ * the das / das_uni kernels tests its element index against the extent of Y
+ * and skips (and counts) a load outside it; the reference's counterpart is
+ * running the CPU code under a memory checker.
+ */
+int dream_das_checked_build(void);
+
+/*
+ * Gather indices outside Y that the bounds-checked build caught for this plan
+ * since it was created (synchronises the device). Always 0 in the normal
+ * build; negative status on error.
+ */
+int64_t dream_das_plan_bound_violations(dream_das_plan *plan);
+
+/*
  * Image-grid hint for the F32_STORE / BF16_STORE kernels: image point n is
  * (n mod n_fast, n / n_fast) on a regular 2-D (or flattened 3-D) grid whose
  * fastest axis has n_fast points, e.g. Nz for Ro = meshgrid(x, z) flattened
