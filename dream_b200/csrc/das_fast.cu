@@ -713,92 +713,125 @@ __device__ __noinline__ int tab_index_exact(const FastParams &P, int64_t n, int 
   return exact_index(P, px, o, i, k) ? k : -1;
 }
 
-__device__ __forceinline__ int tab_index(const FastParams &P, int64_t n, uint64_t s, int64_t colk, int o, int i) {
-  const uint32_t lo = (uint32_t)s;
-  const int32_t kk = (int32_t)((uint32_t)(s >> 32) - (uint32_t)colk);
-  if (lo >= AMB_LO) return (kk >= 0 && kk < P.K) ? kk : (kk == -1 ? 0 : -1);
-  return tab_index_exact(P, n, o, i);
+__device__ __forceinline__ int floor_index(uint64_t s, uint32_t colk, int64_t K) {
+  const int32_t kk = (int32_t)((uint32_t)(s >> 32) - colk);
+  return (kk >= 0 && kk < K) ? kk : (kk == -1 ? 0 : -1);
+}
+
+// Column-owner terms of one image point whose leg sums include an ambiguous
+// one: every term goes through tab_index (floor outside the band, FP64
+// inside). Kept out of line so that the common path holds its arrays in
+// registers. The weight-gradient partials go to the shared accumulator wacc.
+template <bool ADJ, bool WG>
+__device__ __noinline__ void colowner_point_exact(const FastParams &P, const int64_t *__restrict__ TA,
+                                                  const int64_t *__restrict__ TB, int64_t n, int o, int i0, int jn,
+                                                  int n_in, float xn, float gn, float *hist, float *wacc) {
+  const uint64_t A64 = (uint64_t)__ldg(TA + (int64_t)o * P.No + n);
+  const float *Yf = reinterpret_cast<const float *>(P.Y);
+  for (int j = 0; j < jn; j++) {
+    const int64_t col = (int64_t)o * n_in + i0 + j;
+    const uint64_t s = A64 + (uint64_t)__ldg(TB + (int64_t)(i0 + j) * P.No + n);
+    const int k = ((uint32_t)s >= AMB_LO) ? floor_index(s, (uint32_t)(col * P.K), P.K) : tab_index_exact(P, n, o, i0 + j);
+    if (k < 0) continue;
+    if (ADJ) atomicAdd(hist + (int64_t)j * P.K + k, (P.w ? __ldg(P.w + col) : 1.0f) * xn);
+    if (WG) atomicAdd(wacc + j, gn * __ldg(Yf + col * P.K + k));
+  }
 }
 
 // Column-owner adjoint and weight gradient. A CTA owns outer element o and
-// inner elements [i0, i0 + cw), loops over a share of the image points and
+// inner elements [i0, i0 + jn) (jn <= CW), loops over a share of the image
+// points, PX points per thread per step, and
 //   adjoint: Ya[k(n,c), c] += w[c] * X[n]   (shared-memory histogram per column)
 //   wgrad:   dW[c] += G[n] * Y[k(n,c), c]  (per-thread partials, block reduction)
-template <bool ADJ, bool WG>
-__global__ void __launch_bounds__(256) tab_colowner_kernel(const FastParams P, const int64_t *__restrict__ TA,
+// The leg-table loads of the PX points are all issued before any index is
+// formed; an image point with an ambiguous term is handed whole to
+// colowner_point_exact.
+template <bool ADJ, bool WG, int CW, int PX>
+__global__ void __launch_bounds__(256, ADJ ? 4 : 3) tab_colowner_kernel(const FastParams P, const int64_t *__restrict__ TA,
                                                            const int64_t *__restrict__ TB,
                                                            const float *__restrict__ X, const float *__restrict__ G,
-                                                           float *__restrict__ Ya, float *__restrict__ dW, int cw,
-                                                           int splits) {
+                                                           float *__restrict__ Ya, float *__restrict__ dW, int splits) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float *hist = reinterpret_cast<float *>(smem_raw);  // [cw][K] (adjoint)
-  float *red = hist + (ADJ ? (size_t)cw * P.K : 0);   // [cw][warps] (wgrad)
   const int n_in = (P.method == RCA_ROWTX) ? P.Nt : P.Nr;
+  const int jmax = min(CW, n_in);
+  float *hist = reinterpret_cast<float *>(smem_raw);      // [jmax][K] (adjoint)
+  float *red = hist + (ADJ ? (size_t)jmax * P.K : 0);     // [CW][warps] (wgrad)
+  float *wacc = red + (WG ? CW * (blockDim.x >> 5) : 0);  // [CW] (wgrad, exact points)
   const int o = blockIdx.x;
-  const int i0 = blockIdx.y * cw;
-  const int jn = min(cw, n_in - i0);
+  const int i0 = blockIdx.y * CW;
+  const int jn = min(CW, n_in - i0);
   const int split = blockIdx.z;
   const int tid = threadIdx.x, nthr = blockDim.x;
+  const int64_t K = P.K;
   const float *Yf = reinterpret_cast<const float *>(P.Y);
   if (ADJ) {
-    for (int64_t q = tid; q < (int64_t)jn * P.K; q += nthr) hist[q] = 0.0f;
-    __syncthreads();
+    for (int64_t q = tid; q < (int64_t)jn * K; q += nthr) hist[q] = 0.0f;
   }
-  float wsum[16];
+  if (WG && tid < CW) wacc[tid] = 0.0f;
+  __syncthreads();
+  float wc[CW];
+  uint32_t colk[CW];
+  float wsum[CW];
 #pragma unroll
-  for (int j = 0; j < 16; j++) wsum[j] = 0.0f;
-  float wc[16];
-#pragma unroll
-  for (int j = 0; j < 16; j++) wc[j] = (ADJ && j < jn) ? (P.w ? __ldg(P.w + (int64_t)o * n_in + i0 + j) : 1.0f) : 0.0f;
+  for (int j = 0; j < CW; j++) {
+    const int64_t col = (int64_t)o * n_in + i0 + j;
+    wc[j] = (ADJ && j < jn) ? (P.w ? __ldg(P.w + col) : 1.0f) : 0.0f;
+    colk[j] = (uint32_t)(col * K);
+    wsum[j] = 0.0f;
+  }
   const int64_t per = (P.No + splits - 1) / splits;
   const int64_t n0 = (int64_t)split * per, n1 = min(P.No, n0 + per);
-  for (int64_t n = n0 + tid; n < n1; n += nthr) {
-    const uint64_t A64 = (uint64_t)__ldg(TA + (int64_t)o * P.No + n);
-    const float xn = ADJ ? __ldg(X + n) : 0.0f;
-    const float gn = WG ? __ldg(G + n) : 0.0f;
-    // all leg-table loads first, then the indices; the exact path (a call) only
-    // for points whose terms fall in the ambiguity band
-    uint64_t sj[16];
+  const int64_t *ta = TA + (int64_t)o * P.No;
+  const int64_t *tb = TB + (int64_t)i0 * P.No;
+  for (int64_t nb = n0 + tid; nb < n1; nb += (int64_t)PX * nthr) {
+    uint64_t s[PX][CW];
+    float xn[PX], gn[PX];
+    bool on[PX];
 #pragma unroll
-    for (int j = 0; j < 16; j++)
-      sj[j] = (j < jn) ? A64 + (uint64_t)__ldg(TB + (int64_t)(i0 + j) * P.No + n) : 0;
-    uint32_t minlo = 0xffffffffu;
+    for (int q = 0; q < PX; q++) {
+      const int64_t n = nb + (int64_t)q * nthr;
+      on[q] = n < n1;
+      const int64_t nn = on[q] ? n : n0;
+      const uint64_t A64 = (uint64_t)__ldg(ta + nn);
+      xn[q] = ADJ ? __ldg(X + nn) : 0.0f;
+      gn[q] = WG ? __ldg(G + nn) : 0.0f;
 #pragma unroll
-    for (int j = 0; j < 16; j++)
-      if (j < jn) minlo = min(minlo, (uint32_t)sj[j]);
-    int kj[16];
-    if (minlo >= AMB_LO) {
+      for (int j = 0; j < CW; j++) s[q][j] = (j < jn) ? A64 + (uint64_t)__ldg(tb + (int64_t)j * P.No + nn) : ~0ull;
+    }
 #pragma unroll
-      for (int j = 0; j < 16; j++) {
-        const int64_t colk = ((int64_t)o * n_in + i0 + j) * P.K;
-        const int32_t kk = (int32_t)((uint32_t)(sj[j] >> 32) - (uint32_t)colk);
-        kj[j] = (j >= jn) ? -1 : ((kk >= 0 && kk < P.K) ? kk : (kk == -1 ? 0 : -1));
+    for (int q = 0; q < PX; q++) {
+      if (!on[q]) continue;
+      uint32_t minlo = 0xffffffffu;
+#pragma unroll
+      for (int j = 0; j < CW; j++) minlo = min(minlo, (uint32_t)s[q][j]);
+      if (minlo >= AMB_LO) {
+        int k[CW];
+#pragma unroll
+        for (int j = 0; j < CW; j++) k[j] = (j < jn) ? floor_index(s[q][j], colk[j], K) : -1;
+        if (WG) {
+          float yv[CW];
+#pragma unroll
+          for (int j = 0; j < CW; j++) yv[j] = (k[j] >= 0) ? __ldg(Yf + ((int64_t)o * n_in + i0 + j) * K + k[j]) : 0.0f;
+#pragma unroll
+          for (int j = 0; j < CW; j++) wsum[j] = fmaf(gn[q], yv[j], wsum[j]);
+        }
+        if (ADJ) {
+          const float xq = xn[q];
+#pragma unroll
+          for (int j = 0; j < CW; j++)
+            if (k[j] >= 0) atomicAdd(hist + j * K + k[j], wc[j] * xq);
+        }
+      } else {
+        colowner_point_exact<ADJ, WG>(P, TA, TB, nb + (int64_t)q * nthr, o, i0, jn, n_in, xn[q], gn[q], hist, wacc);
       }
-    } else {
-#pragma unroll
-      for (int j = 0; j < 16; j++)
-        kj[j] = (j < jn) ? tab_index(P, n, sj[j], ((int64_t)o * n_in + i0 + j) * P.K, o, i0 + j) : -1;
-    }
-    if (WG) {
-      float yv[16];
-#pragma unroll
-      for (int j = 0; j < 16; j++)
-        yv[j] = (kj[j] >= 0) ? __ldg(Yf + ((int64_t)o * n_in + i0 + j) * P.K + kj[j]) : 0.0f;
-#pragma unroll
-      for (int j = 0; j < 16; j++) wsum[j] = fmaf(gn, yv[j], wsum[j]);
-    }
-    if (ADJ) {
-#pragma unroll
-      for (int j = 0; j < 16; j++)
-        if (kj[j] >= 0) atomicAdd(hist + (int64_t)j * P.K + kj[j], wc[j] * xn);
     }
   }
+  __syncthreads();
   if (ADJ) {
-    __syncthreads();
     for (int j = 0; j < jn; j++) {
-      float *dst = Ya + ((int64_t)o * n_in + i0 + j) * P.K;
-      for (int64_t k = tid; k < P.K; k += nthr) {
-        const float v = hist[(int64_t)j * P.K + k];
+      float *dst = Ya + ((int64_t)o * n_in + i0 + j) * K;
+      for (int64_t k = tid; k < K; k += nthr) {
+        const float v = hist[(int64_t)j * K + k];
         if (splits == 1) dst[k] = v;
         else if (v != 0.0f) atomicAdd(dst + k, v);
       }
@@ -807,14 +840,14 @@ __global__ void __launch_bounds__(256) tab_colowner_kernel(const FastParams P, c
   if (WG) {
     const int lane = tid & 31, warp = tid >> 5, nw = nthr >> 5;
 #pragma unroll
-    for (int j = 0; j < 16; j++) {
+    for (int j = 0; j < CW; j++) {
       float v = wsum[j];
       for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-      if (lane == 0 && j < jn) red[j * nw + warp] = v;
+      if (lane == 0) red[j * nw + warp] = v;
     }
     __syncthreads();
     if (tid < jn) {
-      float v = 0.0f;
+      float v = wacc[tid];
       for (int w = 0; w < nw; w++) v += red[tid * nw + w];
       atomicAdd(dW + (int64_t)o * n_in + i0 + tid, v);
     }
@@ -847,11 +880,45 @@ cudaError_t launch_tab_gather(const FastParams &P, const int64_t *TA, const int6
   return cudaGetLastError();
 }
 
-int colowner_width(int64_t K, int n_in) {
-  int cw = 16;
-  while (cw > 1 && (size_t)cw * K * 4 > 100 * 1024) cw >>= 1;
-  return std::min(cw, n_in);
+// Columns per CTA of the column-owner kernels: a power of two, at most 16
+// for the adjoint (histograms of width x K x 4 bytes within 50 KB, so four
+// CTAs fit on an SM) and 4 for the weight gradient, no wider than the next
+// power of two >= n_in. Narrow CTAs re-read the outer leg table more often
+// but keep more warps resident, which is what these latency-bound loops need
+// (CG configuration: scatter 0.19 ms at width 4 vs 0.26 ms at width 8).
+int colowner_width(int64_t K, int n_in, bool adj) {
+  int cw = adj ? 16 : 4;
+  while (adj && cw > 1 && (size_t)cw * K * 4 > 50 * 1024) cw >>= 1;
+  while (cw > 1 && cw / 2 >= n_in) cw >>= 1;
+  return cw;
 }
+
+namespace {
+
+template <bool ADJ, bool WG, int CW>
+cudaError_t colowner_launch(const FastParams &P, const int64_t *TA, const int64_t *TB, const float *X, const float *G,
+                            float *Ya, float *dW, dim3 grid, size_t smem, int splits, cudaStream_t st) {
+  constexpr int PX = 1;  // two points per thread: more loads in flight but 104 registers, slower
+  cudaError_t e = ensure_smem(tab_colowner_kernel<ADJ, WG, CW, PX>, smem);
+  if (e != cudaSuccess) return e;
+  tab_colowner_kernel<ADJ, WG, CW, PX><<<grid, 256, smem, st>>>(P, TA, TB, X, G, Ya, dW, splits);
+  return cudaGetLastError();
+}
+
+template <bool ADJ, bool WG>
+cudaError_t colowner_dispatch(int cw, const FastParams &P, const int64_t *TA, const int64_t *TB, const float *X,
+                              const float *G, float *Ya, float *dW, dim3 grid, size_t smem, int splits,
+                              cudaStream_t st) {
+  switch (cw) {
+    case 16: return colowner_launch<ADJ, WG, 16>(P, TA, TB, X, G, Ya, dW, grid, smem, splits, st);
+    case 8: return colowner_launch<ADJ, WG, 8>(P, TA, TB, X, G, Ya, dW, grid, smem, splits, st);
+    case 4: return colowner_launch<ADJ, WG, 4>(P, TA, TB, X, G, Ya, dW, grid, smem, splits, st);
+    case 2: return colowner_launch<ADJ, WG, 2>(P, TA, TB, X, G, Ya, dW, grid, smem, splits, st);
+    default: return colowner_launch<ADJ, WG, 1>(P, TA, TB, X, G, Ya, dW, grid, smem, splits, st);
+  }
+}
+
+}  // namespace
 
 cudaError_t launch_tab_colowner(const FastParams &P, const int64_t *TA, const int64_t *TB, const float *X,
                                 const float *G, float *Ya, float *dW, bool adj, bool wg, int sm_count,
@@ -859,27 +926,18 @@ cudaError_t launch_tab_colowner(const FastParams &P, const int64_t *TA, const in
   const int n_out = (P.method == RCA_ROWTX) ? P.Nr : P.Nt;
   const int n_in = (P.method == RCA_ROWTX) ? P.Nt : P.Nr;
   if (n_out == 0 || n_in == 0) return cudaSuccess;
-  int cw = adj ? colowner_width(P.K, n_in) : std::min(16, n_in);
-  if (adj && (size_t)cw * P.K * 4 > 200 * 1024) return cudaErrorInvalidValue;  // A-scans too long for the histogram
+  const int cw = colowner_width(P.K, n_in, adj);
+  const int jmax = std::min(cw, n_in);
+  if (adj && (size_t)jmax * P.K * 4 > 200 * 1024) return cudaErrorInvalidValue;  // A-scans too long for the histogram
   const int groups = (n_in + cw - 1) / cw;
   const int64_t ctas = (int64_t)n_out * groups;
   int splits = (int)std::max<int64_t>(1, std::min<int64_t>(64, (4 * (int64_t)sm_count + ctas - 1) / ctas));
   if (P.No < 4096) splits = 1;
-  const size_t smem = (adj ? (size_t)cw * P.K * 4 : 0) + (wg ? 16 * 8 * 4 : 0);
+  const size_t smem = (adj ? (size_t)jmax * P.K * 4 : 0) + (wg ? (size_t)cw * 8 * 4 + cw * 4 : 0);
   dim3 grid((unsigned)n_out, (unsigned)groups, (unsigned)splits);
-  cudaError_t e;
-  if (adj && wg) {
-    e = ensure_smem(tab_colowner_kernel<true, true>, smem);
-    if (e == cudaSuccess) tab_colowner_kernel<true, true><<<grid, 256, smem, st>>>(P, TA, TB, X, G, Ya, dW, cw, splits);
-  } else if (adj) {
-    e = ensure_smem(tab_colowner_kernel<true, false>, smem);
-    if (e == cudaSuccess) tab_colowner_kernel<true, false><<<grid, 256, smem, st>>>(P, TA, TB, X, G, Ya, dW, cw, splits);
-  } else {
-    e = ensure_smem(tab_colowner_kernel<false, true>, smem);
-    if (e == cudaSuccess) tab_colowner_kernel<false, true><<<grid, 256, smem, st>>>(P, TA, TB, X, G, Ya, dW, cw, splits);
-  }
-  if (e != cudaSuccess) return e;
-  return cudaGetLastError();
+  if (adj && wg) return colowner_dispatch<true, true>(cw, P, TA, TB, X, G, Ya, dW, grid, smem, splits, st);
+  if (adj) return colowner_dispatch<true, false>(cw, P, TA, TB, X, G, Ya, dW, grid, smem, splits, st);
+  return colowner_dispatch<false, true>(cw, P, TA, TB, X, G, Ya, dW, grid, smem, splits, st);
 }
 
 }  // namespace dream

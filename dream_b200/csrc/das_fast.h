@@ -53,7 +53,7 @@ cudaError_t launch_tab_gather(const FastParams &P, const int64_t *TA, const int6
 cudaError_t launch_tab_colowner(const FastParams &P, const int64_t *TA, const int64_t *TB, const float *X,
                                 const float *G, float *Ya, float *dW, bool adj, bool wg, int sm_count,
                                 cudaStream_t st);
-int colowner_width(int64_t K, int n_in);
+int colowner_width(int64_t K, int n_in, bool adj);
 
 // Persistent batch launch over (frame, tile_f index, tile_s index) items
 // (int4: frame, tfi, tsi, unused); resets the queue counter *ctr first.
