@@ -229,19 +229,40 @@ def measure_peaks(dev):
                    "a 32 MiB L2-resident buffer"}
 
 
-def read_traffic(kernel_key: str):
-    """Per-launch DRAM bytes of a kernel from the committed ncu summary."""
+def read_traffic(kernel_key: str, column: int = 1):
+    """Per-launch bytes of a kernel from the committed ncu summary
+    (column 1: DRAM read + write, column 2: L2 -> L1 read bytes)."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     if not os.path.exists(p):
         return None
     for line in open(p):
         parts = line.split()
-        if len(parts) >= 2 and parts[0] == kernel_key and not line.startswith("#"):
+        if len(parts) > column and parts[0] == kernel_key and not line.startswith("#"):
             try:
-                return float(parts[1])
+                return float(parts[column])
             except ValueError:
                 return None
     return None
+
+
+def l2_roofline(sums: int, step_ms: float, peaks: dict) -> dict:
+    """The headline kernel against the measured L2 gather peaks: gathered
+    samples per second against the DAS-shaped gather rate, and L2 -> L1 bytes
+    (ncu, per launch) per second against the random-sector rate."""
+    t = step_ms * 1e-3
+    out = {"achieved_words_per_s": sums / t, "gathered_GBps": sums * 4 / t / 1e9,
+           "peak_das_gather_words_per_s": peaks.get("l2_das_gather_words_per_s"),
+           "peak_l2_random_sector_GBps": peaks.get("l2_random_sector_GBps")}
+    out["frac"] = out["achieved_words_per_s"] / out["peak_das_gather_words_per_s"] \
+        if out["peak_das_gather_words_per_s"] else None
+    l2l1 = read_traffic("das_fast_f32_tfm", 2)
+    out["l2_to_l1_bytes_per_launch"] = l2l1
+    out["l2_to_l1_GBps"] = l2l1 / t / 1e9 if l2l1 else None
+    out["frac_sector"] = out["l2_to_l1_GBps"] / out["peak_l2_random_sector_GBps"] \
+        if (l2l1 and out["peak_l2_random_sector_GBps"]) else None
+    out["note"] = ("frac: samples/s vs the das-shaped gather microbenchmark; frac_sector: L2->L1 sector "
+                   "bytes/s (ncu bytes per launch / live kernel time) vs random 32-byte sector reads")
+    return out
 
 
 def cg_bench(dev, iters: int = 30, reps: int = 3):
@@ -372,6 +393,88 @@ def batch_bench(dev, steps: int = 10, n_frames: int = 48):
             "persistent_ctas": b.grid, "autotune_s": tune_s, "oob_terms": b.oob_count()}
 
 
+CASES = ("fast_f32", "fast_bf16", "plain_f64", "plain_f32", "saft_fast", "saft_plain_f64", "uni_f32",
+         "batch", "op_gather", "op_adjoint", "op_wgrad", "op_backward", "rca_bf16", "rca_f32")
+
+
+def run_case(name: str, repeat: int = 3):
+    """One kernel family on a fixed workload, `repeat` launches after one
+    warm-up, for profiling (`ncu -k <kernel> ... bench.py --case NAME`):
+
+      fast_f32 / fast_bf16 / plain_f64 / plain_f32   TFM 64x64, K=3000, 512x512
+      saft_fast / saft_plain_f64                     SAFT 64 el, K=2048, 256x256
+      uni_f32                                        das_uni TFM 64x64, K=3000, 512x512 (FP32)
+      batch                                          the first 12 of the 48 uneven batch frames
+      op_gather / op_adjoint / op_wgrad / op_backward  CG configuration 32x32, K=2048, 256x256
+      rca_bf16 / rca_f32                             RCA 128x128 row-tx, K=4096, 128x128x256 grid
+    Prints one JSON line with the mean wall time per call (not a bench value)."""
+    import torch
+    from dream_b200 import das, das_f, synth
+    from dream_b200.beamformer import das_mixed, das_uni
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    t = lambda a, dt=np.float64: torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=dt).T)).to(dev).t()
+    if name in ("fast_f32", "fast_bf16", "plain_f64", "plain_f32", "uni_f32"):
+        sc = synth.tfm_scene(seed=1)
+    elif name.startswith("saft"):
+        sc = synth.saft_scene(seed=0)
+    elif name.startswith("op_"):
+        sc = synth.cg_scene(seed=4)
+    else:
+        sc = None
+    if name in ("fast_f32", "fast_bf16"):
+        Y = t(sc.Y, np.float32)
+        fn = lambda: das_mixed(Y, sc.Gt, sc.Gr, sc.Ro, sc.dt, sc.delay, sc.cp, "tfm", "ignore", "cuda:0",
+                               "bf16" if name == "fast_bf16" else "f32")
+    elif name in ("plain_f64", "plain_f32", "saft_plain_f64"):
+        T = np.float32 if name == "plain_f32" else np.float64
+        mod = das_f if T == np.float32 else das
+        method = "saft" if name.startswith("saft") else "tfm"
+        Y, Gt, Ro, dl = t(sc.Y, T), t(sc.Gt, T), t(sc.Ro, T), t(sc.delay, T)
+        Gr = t(sc.Gr, T) if method == "tfm" else None
+        fn = lambda: mod.das(Y, Gt, Gr, Ro, T(sc.dt), dl, T(sc.cp), method, "ignore", "cuda:0")
+    elif name == "saft_fast":
+        Y = t(sc.Y, np.float32)
+        fn = lambda: das_mixed(Y, sc.Gt, None, sc.Ro, sc.dt, sc.delay, sc.cp, "saft", "ignore", "cuda:0", "f32")
+    elif name == "uni_f32":
+        Y = t(sc.Y, np.float32)
+        gt = np.array([sc.Gt[0, 0], sc.Gt[1, 0] - sc.Gt[0, 0], sc.Gt[-1, 0]])
+        xs, zs = np.unique(sc.Ro[:, 0]), np.unique(sc.Ro[:, 2])
+        ro = np.array([[xs[0], xs[1] - xs[0], xs[-1]], [0.0, 1.0, 0.0], [zs[0], zs[1] - zs[0], zs[-1]]])
+        fn = lambda: das_uni(Y, gt, gt, ro, np.float32(sc.dt), 0.0, np.float32(sc.cp), "tfm", "ignore", "cuda:0")
+    elif name == "batch":
+        from dream_b200.batch import DASBatch, make_frame
+        frames = []
+        for sp in synth.batch_specs(7, 48)[:12]:
+            Y, G, Ro, dt, cp = synth.tfm_frame_torch(sp, device=dev)
+            frames.append(make_frame(Y, G, G, Ro, dt, np.zeros((1, 1)), cp, "tfm", device=dev))
+        b = DASBatch(frames, autotune=False)
+        fn = b.run
+    elif name.startswith("op_"):
+        from dream_b200.autograd import DASOperator
+        op = DASOperator(sc.Gt, sc.Gr, sc.Ro, sc.dt, sc.delay, sc.cp, "tfm", 2048, device=dev)
+        x = torch.from_numpy(sc.extra["reflectivity"]).float().to(dev)
+        w = torch.ones(op.ncol, device=dev)
+        Y = op.adjoint(x, w)  # A-scans synthesised from the reflectivity (the CG forward model)
+        fn = {"op_gather": lambda: op.forward(Y, w), "op_adjoint": lambda: op.adjoint(x, w),
+              "op_wgrad": lambda: op.wgrad(x, Y), "op_backward": lambda: op.backward(x, Y, w)}[name]
+    elif name in ("rca_bf16", "rca_f32"):
+        Yr, Gc, Grow, Ro = synth.rca_frame_torch(device=dev)
+        if name == "rca_bf16":
+            Yr = Yr.t().contiguous().to(torch.bfloat16).t()
+        fn = lambda: das_mixed(Yr, Gc, Grow, Ro, 0.025, np.zeros((1, 1)), 1480.0, "rca_rowtx", "ignore",
+                               "cuda:0", "bf16" if name == "rca_bf16" else "f32")
+    else:
+        raise SystemExit(f"unknown case {name!r}; one of {', '.join(CASES)}")
+    fn()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(repeat):
+        fn()
+    torch.cuda.synchronize()
+    print(json.dumps({"case": name, "launches": repeat, "ms_per_call_wall": (time.perf_counter() - t0) * 1e3 / repeat}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -380,7 +483,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--peaks", action="store_true", help="print the measured roofline peaks and exit")
+    ap.add_argument("--case", choices=CASES + ("all",), help="run one kernel family on a fixed workload (profiling)")
+    ap.add_argument("--repeat", type=int, default=3, help="calls of --case after one warm-up call")
     args = ap.parse_args()
+    if args.case:
+        for c in (CASES if args.case == "all" else (args.case,)):
+            run_case(c, args.repeat)
+        return
     if args.impl == "reference":
         return run_reference(args)
     if args.peaks:
@@ -552,11 +661,7 @@ def main():
         "batched": batched,
         "rca": rca,
         "autotuned": {("bf16_store" if k == _lib.PREC_BF16_STORE else "f32_store"): v for k, v in tuned.items()},
-        "roofline_l2": {"achieved_words_per_s": sums / (step_ms * 1e-3),
-                        "peak_das_gather_words_per_s": peaks["l2_das_gather_words_per_s"],
-                        "frac": (sums / (step_ms * 1e-3)) / peaks["l2_das_gather_words_per_s"]
-                        if peaks["l2_das_gather_words_per_s"] else None,
-                        "note": "gathered samples per second against the measured L2 DAS-shaped gather rate"},
+        "roofline_l2": l2_roofline(sums, step_ms, peaks),
         "peaks": peaks,
         "gpu_launches": int(launches_h),
         "clocks": clk,

@@ -3,7 +3,9 @@
 Picks, per shape bucket, the CTA tile of image points (tile_f x tile_s) and
 the inner-chunk length (8 or 16 register-resident legs) by timing each
 candidate on the actual frame with CUDA events (median of a few runs after a
-warm-up). Results are cached in a JSON file keyed by GPU name, method,
+warm-up, the L2 cache flushed before each timed run: a frame that arrives from
+the host or from another kernel is not L2-resident, and shapes that win with
+warm caches can lose without them). Results are cached in a JSON file keyed by GPU name, method,
 storage and bucket, so later processes reuse them:
 
     $DREAM_AUTOTUNE_CACHE or ~/.cache/dream_b200/autotune.json
@@ -63,7 +65,7 @@ def _p2(n: int) -> int:
 def bucket_key(method, storage, Nt, Nr, K, n_fast, No, nthr, device) -> str:
     name = torch.cuda.get_device_name(device).replace(" ", "_")
     n_slow = No // n_fast if n_fast else 1
-    return (f"{name}|{method}|{storage}|nthr={nthr}|Nt={Nt}|Nr={Nr}|K={_p2(K)}|"
+    return (f"v2|{name}|{method}|{storage}|nthr={nthr}|Nt={Nt}|Nr={Nr}|K={_p2(K)}|"
             f"grid={_p2(n_fast) if n_fast else 0}x{_p2(n_slow)}")
 
 
@@ -80,12 +82,16 @@ def candidates(hinted: bool, nthr: int):
     return out
 
 
-def _time_plan(plan_handle, args, reps=5):
+L2_FLUSH_BYTES = 192 << 20  # more than the 126 MB L2
+
+
+def _time_plan(plan_handle, args, flush, reps=5):
     L = _lib.load()
     st = torch.cuda.current_stream()
     L.dream_das_run_device_async(*args)  # warm-up
     ts = []
-    for _ in range(reps):
+    for r in range(reps):
+        flush.fill_(float(r))  # evicts the A-scans from L2
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(st)
         _lib.check(L.dream_das_run_device_async(*args))
@@ -123,15 +129,17 @@ def tune(Y, Gt, Gr, Ro, dt, delay, cp, method="tfm", storage="f32", nthr=None, f
             _lib.DELAY_MULTIPLE if delay.numel() > 1 else _lib.DELAY_SINGLE, ptr(delay), float(cp), ptr(Im),
             ptr(d_oob), ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
     sizes = [nthr] if nthr else [128, 256]
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     best = None
     for n in sizes:
         for tf, ts, jc in candidates(n_fast > 0, n):
             if L.dream_das_set_tile(plan.handle, tf, ts) != 0:
                 continue
             _lib.check(L.dream_das_set_chunk(plan.handle, jc))
-            ms = _time_plan(plan.handle, args)
+            ms = _time_plan(plan.handle, args, flush)
             if best is None or ms < best["ms"]:
                 best = {"tile": [tf, ts], "jc": jc, "n_fast": n_fast, "ms": ms}
+    del flush
     with _lock:
         _load()[key] = best
         _save()

@@ -7,13 +7,20 @@
 // a, b the two FP64 leg times of the reference (extra_src/das.cc:392-404 and
 // its RCA/SAFT counterparts). Each leg is computed exactly once per (pixel,
 // element) in FP64, scaled by Fs in FP64 (A = RN(a*Fs), B = RN(b*Fs)) and
-// stored as fixed point with 24 fraction bits relative to a tile-wide integer
-// base. For A + B the fixed-point sum differs from the exact product
-// RN(RN(a+b)*Fs) by less than 2^-24 + 4 ulp(p), so floor(A + B + delta) with
-// delta = 2^-22 equals the exact floor whenever the fractional part of the
-// shifted sum is at least 2*delta. Terms inside that 2^-21-wide band (about
-// one in a million) take an exact FP64 recomputation. The selected indices
-// are therefore identical to the FP64 plain kernel's.
+// stored as fixed point relative to a tile-wide integer base, in one of two
+// formats chosen per tile:
+//   fine: 24 fraction bits, legs spreading over < 127 samples in the tile;
+//         rounding <= 2^-25 per leg, delta = 2^-22, band 2*delta = 2^-21;
+//   wide: 20 fraction bits (coarse grids, spreads up to 4000 samples);
+//         rounding <= 2^-21 per leg, delta = 2^-19, band 2^-18.
+// For legs below 2^26 samples RN(a*Fs) + RN(b*Fs) differs from
+// RN(RN(a+b)*Fs) by at most 3 ulp(2^27) < 2^-24.4, so in both formats the
+// fixed-point sum is within delta of the exact p, and floor(A + B + delta)
+// equals the exact floor whenever the fractional part of the shifted sum is
+// at least 2*delta. Terms inside the band (about 1 in 2 million with the
+// fine format) take an exact FP64 recomputation. The finer format matters
+// for speed: a warp with one ambiguous lane runs the serial FP64 path. The
+// selected indices are identical to the FP64 plain kernel's.
 //
 // Hot loop. The fixed-point leg carries the A-scan column offset in its high
 // word: with A64 = (offset_t + baseA) << 32 | fraction and the same for B, one
@@ -34,10 +41,17 @@ namespace dream {
 
 namespace {
 
-constexpr int FB = 24;                 // fraction bits of the relative legs
-constexpr uint32_t DELTA_UNITS = 4;    // delta = 2^-22 in 2^-24 units
-constexpr uint32_t AMB_LO = 8u << 8;   // 2*delta in the 2^-32 units of the low word
-constexpr int MAX_EXTENT = 126;        // max integer spread of a leg over a tile
+// Relative fixed-point format of a tile: fb fraction bits, shifted by
+// lo_shift = 32 - fb to the top of the low word of A64 + B64; delta in 2^-fb
+// units; amb_lo = 2*delta in the 2^-32 units of the low word.
+struct FixFmt {
+  int fb, lo_shift;
+  uint32_t delta, amb_lo;
+};
+constexpr FixFmt FMT_FINE{24, 8, 4, 8u << 8};    // delta 2^-22
+constexpr FixFmt FMT_WIDE{20, 12, 2, 4u << 12};  // delta 2^-19
+constexpr int FINE_EXTENT = 126;                 // max integer spread of a leg over a tile, fine format
+constexpr int WIDE_EXTENT = 4000;                // the same, wide format (< 2^12)
 
 template <class YT>
 __device__ __forceinline__ float load_sample(const YT *p);
@@ -59,6 +73,25 @@ __device__ __forceinline__ const YT *elem_addr(const YT *base, uint32_t off) {
   asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(r) : "r"(off), "r"((uint32_t)sizeof(YT)), "l"(base));
   return r;
 }
+
+// Packed FP32 pairs (add.rn.f32x2 / fma.rn.f32x2, sm_100).
+__device__ __forceinline__ uint64_t pack_f32x2(float a, float b) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t add_f32x2(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t fma_f32x2(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+__device__ __forceinline__ float lo_f32(uint64_t v) { return __uint_as_float((uint32_t)v); }
+__device__ __forceinline__ float hi_f32(uint64_t v) { return __uint_as_float((uint32_t)(v >> 32)); }
 
 // Neumaier compensated add of x into (s, c).
 __device__ __forceinline__ void neumaier(float &s, float &c, float x) {
@@ -139,16 +172,16 @@ __device__ __noinline__ bool exact_index(const FastParams &P, const Pixel &px, i
   return false;
 }
 
-// Scaled leg -> integer floor and 24-bit fixed point v = floor << 24 + frac,
-// the same arithmetic wherever a leg is converted. ok = false for legs of
-// 2^26 samples or more: beyond that the FP64 rounding of A + B is no longer
-// far enough below delta, and the tile takes the exact path.
-__device__ __forceinline__ uint32_t fix24(double L, int &fl, bool &ok) {
+// Scaled leg -> integer floor and fixed point v = floor << fb + frac (modulo
+// 2^32), the same arithmetic wherever a leg is converted. ok = false for legs
+// of 2^26 samples or more: beyond that the FP64 rounding of A + B is no
+// longer far enough below delta, and the tile takes the exact path.
+__device__ __forceinline__ uint32_t fix_leg(double L, int fb, int &fl, bool &ok) {
   ok = fabs(L) < 67108864.0;  // 2^26
   double f = floor(ok ? L : 0.0);
   fl = (int)f;
-  uint32_t frac = (uint32_t)__double2uint_rn((L - f) * 16777216.0);  // in [0, 2^24]
-  return ((uint32_t)fl << FB) + frac;
+  uint32_t frac = (uint32_t)__double2uint_rn((L - f) * (double)(1u << fb));  // in [0, 2^fb]
+  return ((uint32_t)fl << fb) + frac;
 }
 
 struct TileShared {
@@ -187,7 +220,7 @@ __device__ __noinline__ float exact_partial(const FastParams &P, const Pixel &px
 template <class YT, bool WEIGHTED, bool CHECKED, bool FULL, int JC, int NO>
 __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &px, const uint64_t (&B64)[JC],
                                              const uint64_t (&A64)[NO], int o0, int i0, int jn, int n_in,
-                                             unsigned int &oob) {
+                                             uint32_t amb_lo, unsigned int &oob) {
   // NO outer elements x JC inner elements: all NO*JC gathers are issued before
   // any (rare) call to the exact path, so they are in flight together.
   const YT *__restrict__ Y = reinterpret_cast<const YT *>(P.Y);
@@ -234,28 +267,31 @@ __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &p
     if (WEIGHTED) {
       const float *w = P.w + (int64_t)(o0 + q) * n_in + i0;
       if (FULL && ((reinterpret_cast<uintptr_t>(w) & 15) == 0)) {
+        uint64_t acc2 = 0;  // (+0, +0)
 #pragma unroll
         for (int j = 0; j < JC; j += 4) {
           float4 w4 = __ldg(reinterpret_cast<const float4 *>(w + j));
-          part = fmaf(w4.x, y[q][j], part);
-          part = fmaf(w4.y, y[q][j + 1], part);
-          part = fmaf(w4.z, y[q][j + 2], part);
-          part = fmaf(w4.w, y[q][j + 3], part);
+          acc2 = fma_f32x2(pack_f32x2(w4.x, w4.y), pack_f32x2(y[q][j], y[q][j + 1]), acc2);
+          acc2 = fma_f32x2(pack_f32x2(w4.z, w4.w), pack_f32x2(y[q][j + 2], y[q][j + 3]), acc2);
         }
+        part = lo_f32(acc2) + hi_f32(acc2);
       } else {
 #pragma unroll
         for (int j = 0; j < JC; j++)
           if (FULL || j < jn) part = fmaf(__ldg(w + j), y[q][j], part);
       }
     } else {
+      // packed FP32x2 adds: half the instructions and half the dependency depth
+      uint64_t acc2 = pack_f32x2(y[q][0], y[q][1]);
 #pragma unroll
-      for (int j = 0; j < JC; j++) part += y[q][j];
+      for (int j = 2; j < JC; j += 2) acc2 = add_f32x2(acc2, pack_f32x2(y[q][j], y[q][j + 1]));
+      part = lo_f32(acc2) + hi_f32(acc2);
     }
     partq[q] = part;
   }
 #pragma unroll
   for (int q = 0; q < NO; q++) {
-    if (minlo[q] < AMB_LO) {
+    if (minlo[q] < amb_lo) {
       // this outer element's partial is replaced by the exact one (which counts its own OOB)
       partq[q] = exact_partial<YT, WEIGHTED>(P, px, o0 + q, i0, jn, n_in, oob);
     } else {
@@ -267,7 +303,8 @@ __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &p
 }
 
 template <class YT, bool WEIGHTED, bool CHECKED, int JC>
-__device__ __forceinline__ void tile_loop(const FastParams &P, const Pixel &px, const TileShared &S, int tid,
+__device__ __forceinline__ void tile_loop(const FastParams &P, const Pixel &px, const TileShared &S, const FixFmt F,
+                                          int tid,
                                           int nthr, int n_out, int n_in, int i_lo, int i_hi, float &acc_s,
                                           float &acc_c, unsigned int &oob) {
   const int64_t K = P.K;
@@ -281,28 +318,28 @@ __device__ __forceinline__ void tile_loop(const FastParams &P, const Pixel &px, 
         const int i = i0 + j;
         int fl;
         bool ok;
-        uint32_t v = fix24(A_mul_Fs(P, inner_leg(P, px, i)), fl, ok);
-        uint32_t brel = v - ((uint32_t)S.minB[i] << FB);
+        uint32_t v = fix_leg(A_mul_Fs(P, inner_leg(P, px, i)), F.fb, fl, ok);
+        uint32_t brel = v - ((uint32_t)S.minB[i] << F.fb);
         uint32_t hi = (uint32_t)(i * K + S.minB[i]);
-        B64[j] = ((uint64_t)brel << 8) + ((uint64_t)hi << 32);
+        B64[j] = ((uint64_t)brel << F.lo_shift) + ((uint64_t)hi << 32);
       }
     }
     if (jn == JC) {
       // compensation every two outer elements (32 terms)
       int o = 0;
       for (; o + 2 <= n_out; o += 2) {
-        const uint64_t A2[2] = {((uint64_t)S.arel[o * nthr + tid] << 8) + ((uint64_t)S.ahi[o] << 32),
-                                ((uint64_t)S.arel[(o + 1) * nthr + tid] << 8) + ((uint64_t)S.ahi[o + 1] << 32)};
-        neumaier(acc_s, acc_c, chunk_terms<YT, WEIGHTED, CHECKED, true, JC, 2>(P, px, B64, A2, o, i0, JC, n_in, oob));
+        const uint64_t A2[2] = {((uint64_t)S.arel[o * nthr + tid] << F.lo_shift) + ((uint64_t)S.ahi[o] << 32),
+                                ((uint64_t)S.arel[(o + 1) * nthr + tid] << F.lo_shift) + ((uint64_t)S.ahi[o + 1] << 32)};
+        neumaier(acc_s, acc_c, chunk_terms<YT, WEIGHTED, CHECKED, true, JC, 2>(P, px, B64, A2, o, i0, JC, n_in, F.amb_lo, oob));
       }
       for (; o < n_out; o++) {
-        const uint64_t A1[1] = {((uint64_t)S.arel[o * nthr + tid] << 8) + ((uint64_t)S.ahi[o] << 32)};
-        neumaier(acc_s, acc_c, chunk_terms<YT, WEIGHTED, CHECKED, true, JC, 1>(P, px, B64, A1, o, i0, JC, n_in, oob));
+        const uint64_t A1[1] = {((uint64_t)S.arel[o * nthr + tid] << F.lo_shift) + ((uint64_t)S.ahi[o] << 32)};
+        neumaier(acc_s, acc_c, chunk_terms<YT, WEIGHTED, CHECKED, true, JC, 1>(P, px, B64, A1, o, i0, JC, n_in, F.amb_lo, oob));
       }
     } else {
       for (int o = 0; o < n_out; o++) {
-        const uint64_t A1[1] = {((uint64_t)S.arel[o * nthr + tid] << 8) + ((uint64_t)S.ahi[o] << 32)};
-        neumaier(acc_s, acc_c, chunk_terms<YT, WEIGHTED, CHECKED, false, JC, 1>(P, px, B64, A1, o, i0, jn, n_in, oob));
+        const uint64_t A1[1] = {((uint64_t)S.arel[o * nthr + tid] << F.lo_shift) + ((uint64_t)S.ahi[o] << 32)};
+        neumaier(acc_s, acc_c, chunk_terms<YT, WEIGHTED, CHECKED, false, JC, 1>(P, px, B64, A1, o, i0, jn, n_in, F.amb_lo, oob));
       }
     }
   }
@@ -361,7 +398,7 @@ __device__ __forceinline__ void fast_tile(const FastParams &P, int64_t tfi, int6
   for (int o = 0; o < n_out; o++) {
     int fl;
     bool ok;
-    uint32_t v = fix24(A_mul_Fs(P, outer_leg(P, px, o)), fl, ok);
+    uint32_t v = fix_leg(A_mul_Fs(P, outer_leg(P, px, o)), FMT_FINE.fb, fl, ok);
     bad |= !ok;
     S.arel[o * nthr + tid] = v;
     int mn = __reduce_min_sync(0xffffffffu, fl), mx = __reduce_max_sync(0xffffffffu, fl);
@@ -373,7 +410,7 @@ __device__ __forceinline__ void fast_tile(const FastParams &P, int64_t tfi, int6
   for (int i = i_lo; i < i_hi; i++) {
     int fl;
     bool ok;
-    fix24(A_mul_Fs(P, inner_leg(P, px, i)), fl, ok);
+    fix_leg(A_mul_Fs(P, inner_leg(P, px, i)), FMT_FINE.fb, fl, ok);
     bad |= !ok;
     int mn = __reduce_min_sync(0xffffffffu, fl), mx = __reduce_max_sync(0xffffffffu, fl);
     if (lane == 0) {
@@ -396,8 +433,8 @@ __device__ __forceinline__ void fast_tile(const FastParams &P, int64_t tfi, int6
     loB = min(loB, S.minB[i]);
     hiB = max(hiB, S.maxB[i]);
   }
-  const bool exact_tile = S.flags[0] != 0 || ext > MAX_EXTENT ||
-                          (int64_t)n_out * n_in * P.K + (int64_t)hiA + hiB + 256 >= (int64_t(1) << 32) ||
+  const bool exact_tile = S.flags[0] != 0 || ext > WIDE_EXTENT ||
+                          (int64_t)n_out * n_in * P.K + (int64_t)hiA + hiB + 8448 >= (int64_t(1) << 32) ||
                           (int64_t)loA + loB < -(int64_t(1) << 30);
   // a non-ambiguous term's floor index lies in [minA + minB, maxA + maxB + 2]
   const bool in_bounds = (int64_t)loA + loB >= 0 && (int64_t)hiA + hiB + 2 < P.K;
@@ -422,15 +459,24 @@ __device__ __forceinline__ void fast_tile(const FastParams &P, int64_t tfi, int6
       neumaier(acc_s, acc_c, part);
     }
   } else {
-    // rebase the outer legs on the tile minimum and add the delta shift
-    for (int o = 0; o < n_out; o++)
-      S.arel[o * nthr + tid] = S.arel[o * nthr + tid] - ((uint32_t)S.minA[o] << FB) + DELTA_UNITS;
+    // format of this tile; rebase the outer legs on the tile minimum and add
+    // the delta shift (the wide format converts the outer legs again)
+    const FixFmt F = ext > FINE_EXTENT ? FMT_WIDE : FMT_FINE;
+    for (int o = 0; o < n_out; o++) {
+      uint32_t v = S.arel[o * nthr + tid];
+      if (F.fb != FMT_FINE.fb) {
+        int fl;
+        bool ok;
+        v = fix_leg(A_mul_Fs(P, outer_leg(P, px, o)), F.fb, fl, ok);
+      }
+      S.arel[o * nthr + tid] = v - ((uint32_t)S.minA[o] << F.fb) + F.delta;
+    }
     for (int o = tid; o < n_out; o += nthr) S.ahi[o] = (uint32_t)((int64_t)o * n_in * P.K + S.minA[o]);
     __syncthreads();
     if (in_bounds)
-      tile_loop<YT, WEIGHTED, false, JC>(P, px, S, tid, nthr, n_out, n_in, i_lo, i_hi, acc_s, acc_c, oob);
+      tile_loop<YT, WEIGHTED, false, JC>(P, px, S, F, tid, nthr, n_out, n_in, i_lo, i_hi, acc_s, acc_c, oob);
     else
-      tile_loop<YT, WEIGHTED, true, JC>(P, px, S, tid, nthr, n_out, n_in, i_lo, i_hi, acc_s, acc_c, oob);
+      tile_loop<YT, WEIGHTED, true, JC>(P, px, S, F, tid, nthr, n_out, n_in, i_lo, i_hi, acc_s, acc_c, oob);
   }
   if (active) P.Im[no] = P.accumulate ? P.Im[no] + (acc_s + acc_c) : acc_s + acc_c;
   add_count(P.oob, active ? oob : 0u);
@@ -613,7 +659,8 @@ cudaError_t convert_f32_to_bf16(const float *x, void *y, int64_t n, cudaStream_t
 
 namespace {
 
-constexpr uint32_t TAB_DELTA = 1u << 10;  // 2^-22 in 2^-32 units
+constexpr uint32_t TAB_DELTA = 1u << 10;       // 2^-22 in 2^-32 units
+constexpr uint32_t TAB_AMB_LO = 2 * TAB_DELTA;  // ambiguity band of the table terms
 
 __global__ void legtab_kernel(const FastParams P, int64_t *__restrict__ TA, int64_t *__restrict__ TB,
                               int *__restrict__ range) {
@@ -667,8 +714,9 @@ __device__ __forceinline__ void tab_gather_body(const FastParams &P, const Pixel
     for (int j = 0; j < JC; j++) B64[j] = (j < jn) ? (uint64_t)__ldg(TB + (int64_t)(i0 + j) * P.No + n) : 0;
     for (int o = 0; o < n_out; o++) {
       const uint64_t A1[1] = {(uint64_t)__ldg(TA + (int64_t)o * P.No + n)};
-      float part = (jn == JC) ? chunk_terms<YT, WEIGHTED, CHECKED, true, JC, 1>(P, px, B64, A1, o, i0, JC, n_in, oob)
-                              : chunk_terms<YT, WEIGHTED, CHECKED, false, JC, 1>(P, px, B64, A1, o, i0, jn, n_in, oob);
+      float part =
+          (jn == JC) ? chunk_terms<YT, WEIGHTED, CHECKED, true, JC, 1>(P, px, B64, A1, o, i0, JC, n_in, TAB_AMB_LO, oob)
+                     : chunk_terms<YT, WEIGHTED, CHECKED, false, JC, 1>(P, px, B64, A1, o, i0, jn, n_in, TAB_AMB_LO, oob);
       neumaier(acc_s, acc_c, part);
     }
   }
@@ -731,7 +779,7 @@ __device__ __noinline__ void colowner_point_exact(const FastParams &P, const int
   for (int j = 0; j < jn; j++) {
     const int64_t col = (int64_t)o * n_in + i0 + j;
     const uint64_t s = A64 + (uint64_t)__ldg(TB + (int64_t)(i0 + j) * P.No + n);
-    const int k = ((uint32_t)s >= AMB_LO) ? floor_index(s, (uint32_t)(col * P.K), P.K) : tab_index_exact(P, n, o, i0 + j);
+    const int k = ((uint32_t)s >= TAB_AMB_LO) ? floor_index(s, (uint32_t)(col * P.K), P.K) : tab_index_exact(P, n, o, i0 + j);
     if (k < 0) continue;
     if (ADJ) atomicAdd(hist + (int64_t)j * P.K + k, (P.w ? __ldg(P.w + col) : 1.0f) * xn);
     if (WG) atomicAdd(wacc + j, gn * __ldg(Yf + col * P.K + k));
@@ -804,7 +852,7 @@ __global__ void __launch_bounds__(256, ADJ ? 4 : 3) tab_colowner_kernel(const Fa
       uint32_t minlo = 0xffffffffu;
 #pragma unroll
       for (int j = 0; j < CW; j++) minlo = min(minlo, (uint32_t)s[q][j]);
-      if (minlo >= AMB_LO) {
+      if (minlo >= TAB_AMB_LO) {
         int k[CW];
 #pragma unroll
         for (int j = 0; j < CW; j++) k[j] = (j < jn) ? floor_index(s[q][j], colk[j], K) : -1;

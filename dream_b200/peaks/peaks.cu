@@ -6,7 +6,8 @@
 //                     an L2-resident buffer: 32 sectors per warp request
 //   l2_das_gather     the DAS access shape: each warp reads 32 words spread
 //                     over a window of ~100 words at a random offset
-//   fp32_fma, fp64_fma, int_add   dependent-chain-free arithmetic throughput
+//   fp32_fma, fp64_fma, int_add   arithmetic throughput over 8 independent chains
+//                     per thread (int_add counts the XOR and the ADD of each step)
 //
 // Each kernel returns nothing useful; results are derived from CUDA-event
 // time and the known operation counts.
@@ -87,7 +88,7 @@ __global__ void int_add(int iters, float *__restrict__ sink) {
   for (int j = 0; j < 8; j++) a[j] = threadIdx.x + j;
   for (int r = 0; r < iters; r++) {
 #pragma unroll
-    for (int j = 0; j < 8; j++) a[j] = a[j] + (a[(j + 1) & 7] ^ 0x5bd1e995u);
+    for (int j = 0; j < 8; j++) a[j] = (a[j] ^ 0x5bd1e995u) + 0x9e3779b9u;  // two ALU operations, 8 chains
   }
   uint32_t s = 0;
 #pragma unroll
@@ -124,7 +125,7 @@ double dream_peaks_run(int kind, const float *buf, int log2_words, int blocks, i
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   const double n = (double)blocks * threads * iters;
-  *ops = (kind <= 1) ? n : n * 8.0;
+  *ops = (kind <= 1) ? n : (kind == 4 ? n * 16.0 : n * 8.0);
   return cudaGetLastError() == cudaSuccess ? (double)ms : -4.0;
 }
 

@@ -54,6 +54,24 @@ def test_index_reveal_fp64_indices(hint, grid):
     assert np.array_equal(Im.astype(np.int64) - 1, k)
 
 
+@pytest.mark.parametrize("tile", [None, (32, 8), (8, 32)])
+@pytest.mark.parametrize("grid", [
+    (24, 40, (-20.0, 20.0), (0.0, 50.0), 3000),     # ~43 samples between z neighbours: wide tiles, fast path
+    (8, 8, (-20.0, 20.0), (0.0, 400.0), 14000),     # ~1900 samples between neighbours: beyond 4000 per tile
+])
+def test_index_reveal_coarse_grids(grid, tile):
+    """Coarse grids put a leg's samples far apart within one tile (hundreds to
+    thousands of samples): the relative fixed point must still select the
+    FP64 indices, and tiles spreading beyond its range take the exact path."""
+    nx, nz, xr, zr, K = grid
+    s = _index_reveal(K=K, nx=nx, nz=nz, x_rng=xr, z_rng=zr)
+    _, _, _, idx = oracle.das(s.Y, s.Gt, s.Gr, s.Ro, s.dt, s.delay, s.cp, "tfm", "ignore", np.float64,
+                              return_idx=True)
+    Im = mixed(s, tile=tile)
+    k = np.where(idx[0] == oracle.OOB_MISS, -1, idx[0])
+    assert np.array_equal(Im.astype(np.int64) - 1, k)
+
+
 @pytest.mark.parametrize("delay", [-0.03, -0.045, 0.0])
 def test_near_element_truncation(delay):
     s = _near_element(delay)
