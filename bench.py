@@ -425,7 +425,7 @@ def run_case(name: str, repeat: int = 3):
     if name in ("fast_f32", "fast_bf16"):
         Y = t(sc.Y, np.float32)
         fn = lambda: das_mixed(Y, sc.Gt, sc.Gr, sc.Ro, sc.dt, sc.delay, sc.cp, "tfm", "ignore", "cuda:0",
-                               "bf16" if name == "fast_bf16" else "f32")
+                               "bf16" if name == "fast_bf16" else "f32", tile=(16, 8))  # the autotuned tile
     elif name in ("plain_f64", "plain_f32", "saft_plain_f64"):
         T = np.float32 if name == "plain_f32" else np.float64
         mod = das_f if T == np.float32 else das
