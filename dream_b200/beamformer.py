@@ -74,9 +74,10 @@ def _plan(key, create):
     if cache is None:
         cache = _tls.plans = {}
     p = cache.get(key[0])
-    if p is None or p.key != key:
+    if p is None or getattr(p, "cache_key", None) != key:
         cache.pop(key[0], None)
         p = create()
+        p.cache_key = key  # the plan is reused while calls bring the same key
         cache[key[0]] = p
     return p
 
@@ -307,6 +308,35 @@ def _fast_plan(das_type, K, No, Nt, Nr, prec, dev, hint, tile=None):
     return plan
 
 
+def _das_mixed_host(Y, Gt, Gr, Ro, dt, delay, cp, das_type, level, dev, prec, hint, tile):
+    """Host arrays through the C ABI's host entry (dream_das_run): FP32
+    A-scans, FP64 geometry, column-major. For TFM and RCA frames of 8 MB or
+    more the library uploads the A-scans in chunks of inner elements on a copy
+    stream and beamforms each chunk as it lands, so the upload (the larger part
+    of an end-to-end call) overlaps the kernels; pinned host memory makes the
+    copies run at full link speed."""
+    host = lambda a: a.numpy() if _is_torch(a) else a
+    Yh = _fortran(host(Y), np.float32)
+    Gth = _fortran(host(Gt), np.float64)
+    Grh = _fortran(host(Gr), np.float64) if Gr is not None and das_type != _lib.SAFT else None
+    Roh = _fortran(host(Ro), np.float64)
+    dlh = _fortran(host(delay), np.float64)
+    if Yh.ndim == 1:
+        Yh = Yh.reshape(-1, 1, order="F")
+    K, No, Nt, Nr, multi = _check_shapes(Yh, Gth, Grh, Roh, dlh, das_type)
+    h = grid_hint(Roh) if hint == "auto" else int(hint or 0)
+    plan = _fast_plan(das_type, K, No, Nt, Nr, prec, dev, h, tile)
+    out = np.empty(No, dtype=np.float32)
+    ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p) if a is not None and a.size else None
+    oob = ctypes.c_int64(0)
+    st = _lib.check(_lib.load().dream_das_run(
+        plan.handle, ptr(Yh), ptr(Roh), ptr(Gth), ptr(Grh), float(dt),
+        _lib.DELAY_MULTIPLE if multi else _lib.DELAY_SINGLE, ptr(dlh), float(cp), ptr(out), level,
+        ctypes.byref(oob)))
+    _report(st)
+    return out
+
+
 def das_mixed(Y, Gt, Gr, Ro, dt, delay, cp, method, err_level="stop", device="cuda", storage="f32",
               weights=None, hint="auto", tile=None, stream=None):
     """DAS with A-scans stored in FP32 (``storage='f32'``) or BF16 and FP32
@@ -322,6 +352,8 @@ def das_mixed(Y, Gt, Gr, Ro, dt, delay, cp, method, err_level="stop", device="cu
     dev = parse_device(device)
     prec = _STORAGE[storage]
     on_host = not (_is_torch(Y) and Y.device.type == "cuda")
+    if on_host and weights is None and stream is None:
+        return _das_mixed_host(Y, Gt, Gr, Ro, dt, delay, cp, das_type, level, dev, prec, hint, tile)
     device_t = Y.device if not on_host else torch.device("cuda", dev)
     dev = device_t.index if device_t.index is not None else torch.cuda.current_device()
     ydt = np.float32

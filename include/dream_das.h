@@ -211,6 +211,17 @@ int dream_das_get_tile(const dream_das_plan *plan, int *tile_f, int *tile_s);
 int dream_das_set_chunk(dream_das_plan *plan, int jc);
 
 /*
+ * L2 blocking of the F32_STORE / BF16_STORE kernels (TFM, RCA; no counterpart
+ * in the reference, whose CPU loops have no such cache to fit). A-scans larger
+ * than the budget are beamformed in passes over ranges of inner elements (a
+ * multiple of 16 each) whose A-scans take at most `bytes`, each pass adding
+ * into the image: the pass's samples stay in L2 while every image point
+ * gathers from them. 0 = automatic (passes of at most 96 MB when the A-scans
+ * exceed 160 MB), < 0 = never split. The image changes only by FP32 rounding.
+ */
+int dream_das_set_l2_block(dream_das_plan *plan, int64_t bytes);
+
+/*
  * Weighted DAS, the forward operator of the differentiable beamformer:
  *   Im[n] = sum over A-scan columns c of w[c] * Y[k(n, c), c]
  * with k the FP64-exact sample index of the plain method. F32_STORE and

@@ -94,3 +94,45 @@ def test_method_aliases_and_saft_ignores_gr():
                                                     np.zeros((4, 3)), np.zeros((4, 1)), _lib.SAFT)
     assert (K, No, Nt, Nr, multi) == (10, 4, 2, 0, True)
     assert beamformer.parse_device("cuda:3") == 3 and beamformer.parse_device("gpu") == 0
+
+
+def test_plan_cache_reuses_plans_per_key():
+    """Bindings keep one plan per kind and thread while calls bring the same
+    setup (das_setup_has_changed, include/das.h:77-94): a plan is created once
+    per key, not on every call, and replaced when the setup changes."""
+    import threading
+
+    from dream_b200 import beamformer
+
+    class FakePlan:
+        created = 0
+
+        def __init__(self):
+            FakePlan.created += 1
+
+    def run():
+        beamformer._tls.__dict__.pop("plans", None)
+        k1 = ("fast", 1, 3000, 262144, 64, 64, 2, 0)
+        k2 = ("fast", 1, 3000, 262144, 64, 64, 3, 0)
+        a = beamformer._plan(k1, FakePlan)
+        assert beamformer._plan(k1, FakePlan) is a and FakePlan.created == 1
+        b = beamformer._plan(k2, FakePlan)
+        assert b is not a and FakePlan.created == 2
+        assert beamformer._plan(k2, FakePlan) is b and FakePlan.created == 2
+        c = beamformer._plan(("das",) + k1[1:], FakePlan)  # another kind keeps its own slot
+        assert beamformer._plan(k2, FakePlan) is b and c is not b and FakePlan.created == 3
+
+    errors = []
+
+    def guarded():
+        try:
+            run()
+        except Exception as e:  # surfaced below: assertions in a thread do not fail the test
+            errors.append(e)
+
+    t = threading.Thread(target=guarded)  # a fresh thread-local cache
+    t.start()
+    t.join()
+    if errors:
+        raise errors[0]
+    assert FakePlan.created == 3
