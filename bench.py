@@ -361,6 +361,70 @@ def rca_bench(dev, steps: int = 3):
     return out
 
 
+def conv_bench(dev, cpu_sample: bool = True):
+    """A-scan synthesis of the reference's TFM test (python/tests/test_das_tfm.py:
+    97-105) on the GPU: 101 elements, 2000-sample spatial impulse responses H
+    (seeded stand-ins), 150-sample pulse at 50 MHz; per transmit t,
+    Hdp = fftconv_p(H, H[:, t]) then Y[:, t*101:(t+1)*101] = conv(Hdp, pulse):
+    4.69e10 FP64 multiply-adds, bit-identical to the reference's direct conv().
+    Device-resident inputs, CUDA events around all 202 launches."""
+    import torch
+    from dream_b200.conv import conv_p, fftconv_p
+    L, nt, nt_he = 101, 2000, 150
+    rng = np.random.default_rng(21)
+    H = torch.from_numpy(np.ascontiguousarray(rng.normal(size=(L, nt)))).to(dev).t()  # column-major
+    t = np.arange(nt_he) / 50.0
+    h_e = torch.from_numpy(-np.exp(-10.0 * (t - 0.55) ** 2) * np.cos(2 * np.pi * 2.5 * t)).to(dev)
+    Yfmc = torch.empty((L * L, 2 * nt - 1 + nt_he - 1), dtype=torch.float64, device=dev).t()
+
+    def synth():
+        for n_t in range(L):
+            Hdp = fftconv_p(H, H[:, n_t])
+            conv_p(Hdp, h_e, Yfmc[:, n_t * L:(n_t + 1) * L], "=")
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms = []
+        for _ in range(3):
+            a.record()
+            fn()
+            e.record()
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(e))
+        return min(ms)
+
+    ms_eager = timed(synth)
+    # the same 202 launches captured once in a CUDA graph: device time without
+    # the per-call host work of the Python front end
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(side):
+        synth()
+    torch.cuda.current_stream(dev).wait_stream(side)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        synth()
+    ms = timed(g.replay)
+    macs = L * (nt * nt * L + (2 * nt - 1) * nt_he * L)
+    out = {"config": "FMC synthesis, 101 elements, SIR 2000 samples, pulse 150 samples, FP64 (reference TFM test)",
+           "macs": macs, "ms": ms, "gmac_s": macs / ms / 1e6, "ms_eager": ms_eager,
+           "note": "bit-identical to the reference's direct conv(); FFTW's fftconv_p differs by rounding; "
+                   "ms: the 202 launches replayed from a CUDA graph, ms_eager: issued from Python"}
+    if cpu_sample:
+        from oracle import oracle
+        Hh = np.asfortranarray(H.cpu().numpy())
+        t0 = time.perf_counter()
+        Hdp = oracle.conv_p(Hh, Hh[:, 0])
+        oracle.conv_p(Hdp, h_e.cpu().numpy())
+        dt_cpu = time.perf_counter() - t0
+        out["cpu_port"] = {"gmac_s": (macs / L) / dt_cpu / 1e9, "cores": 1, "kind": "port",
+                           "sample": "one transmit (4.65e8 multiply-adds) through oracle/conv_oracle.c; the "
+                                     "reference's FFTW-based fftconv_p cannot be built here (no FFTW headers)"}
+    return out
+
+
 def batch_bench(dev, steps: int = 10, n_frames: int = 48):
     """48 uneven TFM frames (elements from {16,32,64,128}, K ~ U{1024..4096},
     cp ~ U[1450,1550], grids 64^2..512^2), FP32, one persistent launch captured
@@ -394,7 +458,7 @@ def batch_bench(dev, steps: int = 10, n_frames: int = 48):
 
 
 CASES = ("fast_f32", "fast_bf16", "plain_f64", "plain_f32", "saft_fast", "saft_plain_f64", "uni_f32",
-         "batch", "op_gather", "op_adjoint", "op_wgrad", "op_backward", "rca_bf16", "rca_f32")
+         "batch", "op_gather", "op_adjoint", "op_wgrad", "op_backward", "rca_bf16", "rca_f32", "conv_dp", "conv_pulse")
 
 
 def run_case(name: str, repeat: int = 3):
@@ -407,6 +471,8 @@ def run_case(name: str, repeat: int = 3):
       batch                                          the first 12 of the 48 uneven batch frames
       op_gather / op_adjoint / op_wgrad / op_backward  CG configuration 32x32, K=2048, 256x256
       rca_bf16 / rca_f32                             RCA 128x128 row-tx, K=4096, 128x128x256 grid
+      conv_dp / conv_pulse                           fftconv_p of the TFM synthesis: 2000x101 SIRs with a
+                                                     2000-sample column / 3999x101 with the 150-sample pulse
     Prints one JSON line with the mean wall time per call (not a bench value)."""
     import torch
     from dream_b200 import das, das_f, synth
@@ -464,6 +530,13 @@ def run_case(name: str, repeat: int = 3):
             Yr = Yr.t().contiguous().to(torch.bfloat16).t()
         fn = lambda: das_mixed(Yr, Gc, Grow, Ro, 0.025, np.zeros((1, 1)), 1480.0, "rca_rowtx", "ignore",
                                "cuda:0", "bf16" if name == "rca_bf16" else "f32")
+    elif name in ("conv_dp", "conv_pulse"):
+        from dream_b200.conv import fftconv_p
+        rng = np.random.default_rng(21)
+        M, Lp = (2000, 2000) if name == "conv_dp" else (3999, 150)
+        A = torch.from_numpy(np.ascontiguousarray(rng.normal(size=(101, M)))).to(dev).t()
+        B = torch.from_numpy(rng.normal(size=Lp)).to(dev)
+        fn = lambda: fftconv_p(A, B)
     else:
         raise SystemExit(f"unknown case {name!r}; one of {', '.join(CASES)}")
     fn()
@@ -628,6 +701,7 @@ def main():
     cg = cg_bench(dev)
     batched = batch_bench(dev)
     rca = rca_bench(dev)
+    conv = conv_bench(dev, cpu_sample=(rank == 0 and not args.no_cpu_baseline))
     peaks = measure_peaks(dev)
 
     if world > 1:
@@ -660,6 +734,7 @@ def main():
         "adjoint_cg": cg,
         "batched": batched,
         "rca": rca,
+        "conv_fmc": conv,
         "autotuned": {("bf16_store" if k == _lib.PREC_BF16_STORE else "f32_store"): v for k, v in tuned.items()},
         "roofline_l2": l2_roofline(sums, step_ms, peaks),
         "peaks": peaks,

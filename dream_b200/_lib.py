@@ -29,6 +29,7 @@ ERR_CANCELLED = -5
 SAFT, TFM, RCA_COLTX, RCA_ROWTX = 0, 1, 2, 3
 LVL_NONE, LVL_IGNORE, LVL_WARN, LVL_STOP = 0, 1, 2, 3
 DELAY_SINGLE, DELAY_MULTIPLE = 0, 1
+CONV_EQU, CONV_SUM, CONV_NEG = 0, 1, 2
 PREC_F64, PREC_F32, PREC_F32_STORE, PREC_BF16_STORE = 0, 1, 2, 3
 
 # every symbol include/dream_das.h declares: name -> (restype, argtypes)
@@ -57,6 +58,8 @@ SIGNATURES = {
     "dream_das_set_tile": (_i, [_vp, _i, _i]),
     "dream_das_set_chunk": (_i, [_vp, _i]),
     "dream_das_set_l2_block": (_i, [_vp, _i64]),
+    "dream_conv_p_run_device": (_i, [_vp, _i64, _i64, _vp, _i64, _i64, _vp, _i, _vp]),
+    "dream_conv_p_run": (_i, [_vp, _i64, _i64, _vp, _i64, _i64, _vp, _i, _i]),
     "dream_das_get_tile": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "dream_das_weighted_run_device": (_i, [_vp, _vp, _vp, _vp, _vp, _d, _i, _vp, _d, _vp, _vp, _vp, _vp]),
     "dream_das_bind_geometry": (_i, [_vp, _vp, _vp, _vp, _d, _i, _vp, _d, _vp]),

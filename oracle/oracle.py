@@ -29,9 +29,9 @@ _lib = None
 
 
 def build() -> str:
-    """Compiles das_oracle.c with gcc (make) if the shared object is stale."""
-    src = os.path.join(HERE, "das_oracle.c")
-    if (not os.path.exists(LIB_PATH)) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+    """Compiles das_oracle.c and conv_oracle.c with gcc (make) if the shared object is stale."""
+    srcs = [os.path.join(HERE, f) for f in ("das_oracle.c", "conv_oracle.c")]
+    if (not os.path.exists(LIB_PATH)) or os.path.getmtime(LIB_PATH) < max(os.path.getmtime(f) for f in srcs):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB_PATH
 
@@ -56,6 +56,8 @@ def lib():
         for n in ("dream_oracle_das_weighted_f64", "dream_oracle_das_adjoint_f64"):
             getattr(L, n).argtypes = [vp, i64, i64, i64, vp, vp, vp]
         L.dream_oracle_das_wgrad_f64.argtypes = [vp, i64, i64, i64, vp, vp, vp]
+        L.dream_oracle_conv_p.argtypes = [vp, i64, i64, vp, i64, i64, vp, i32]
+        L.dream_oracle_conv_p.restype = None
         _lib = L
     return _lib
 
@@ -172,3 +174,29 @@ def reference_module(precision: str = "f64"):
     mod = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mod)
     return mod
+
+
+CONV_MODES = {"=": 0, "+=": 1, "-=": 2}
+
+
+def conv_p(A, B, Y=None, mode="="):
+    """Column-wise full linear convolution, the direct form of the reference's
+    conv() (conv_oracle.c; parity unpinned: the reference needs FFTW to build).
+    Returns Y ((A_M + B_M - 1) x A_N, FP64, column-major); with Y given it is
+    updated in place by mode '=', '+=' or '-='."""
+    A = np.asfortranarray(np.asarray(A, dtype=np.float64))
+    B = np.asfortranarray(np.asarray(B, dtype=np.float64))
+    if A.ndim == 1:
+        A = A.reshape(-1, 1, order="F")
+    A_M, A_N = A.shape
+    B_M, B_N = (B.shape[0], B.shape[1]) if B.ndim == 2 else (B.shape[0], 1)
+    if B_M == 1 or B_N == 1:
+        B_M, B_N = B_M * B_N, 1
+    elif B_N != A_N:
+        raise RuntimeError("Argument 2 must be a vector or a matrix with the same number of columns as arg 1!")
+    if Y is None:
+        Y = np.zeros((A_M + B_M - 1, A_N), dtype=np.float64, order="F")
+    assert Y.flags["F_CONTIGUOUS"] and Y.dtype == np.float64 and Y.shape == (A_M + B_M - 1, A_N)
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    lib().dream_oracle_conv_p(p(A), A_M, A_N, p(B), B_M, B_N, p(Y), CONV_MODES[mode])
+    return Y
