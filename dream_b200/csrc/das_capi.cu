@@ -889,6 +889,73 @@ static int run_device_impl(dream_das_plan *p, const void *dY, const void *dRo, c
   return launch_plain(p, L, st);
 }
 
+int dream_das_indices_device(dream_das_plan *p, const void *dRo, const void *dGt, const void *dGr, double dt,
+                             int delay_type, const void *ddelay, double cp, int64_t *d_idx, int64_t *oob_count,
+                             void *stream) {
+  if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
+  if (p->uni) return fail(DREAM_ERR_ARGUMENT, "uniform-grid plan passed to dream_das_indices_device");
+  if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
+  if (delay_type != DREAM_DELAY_SINGLE && delay_type != DREAM_DELAY_MULTIPLE)
+    return fail(DREAM_ERR_ARGUMENT, "unknown delay type");
+  if (ddelay == nullptr) return fail(DREAM_ERR_ARGUMENT, "delay pointer is NULL");
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  // F32 plans: das_f's FP32 indices; every other precision: das's FP64 ones
+  // (the indices the FP32/BF16-storage kernels select as well)
+  const bool f32 = p->precision == DREAM_PREC_F32;
+  PlainLaunch L;
+  memset(&L, 0, sizeof(L));
+  L.method = effective_method(p);
+  L.K = p->K;
+  L.Ro = dRo;
+  L.No = p->No;
+  L.Gt = dGt;
+  L.Nt = p->Nt;
+  L.Gr = dGr;
+  L.Nr = (L.method == DREAM_DAS_SAFT) ? 0 : p->Nr;
+  L.delay_vec = ddelay;
+  L.delay_multi = delay_type == DREAM_DELAY_MULTIPLE;
+  if (f32) L.c32 = constants_das_f32((float)dt, (float)cp, 0.0f);
+  else L.c64 = constants_f64(dt, cp, 0.0);
+  if (L.method >= DREAM_DAS_RCA_COLTX) {
+    int r = check_rca_edges(p->Nt, p->Nr);
+    if (r) return r;
+  }
+  const int64_t terms = terms_per_pixel(p);
+  if (p->No == 0 || terms == 0) {
+    if (oob_count) *oob_count = 0;
+    return 0;
+  }
+  if (dRo == nullptr || dGt == nullptr || d_idx == nullptr || (L.Nr > 0 && dGr == nullptr))
+    return fail(DREAM_ERR_ARGUMENT, "NULL device pointer");
+  unsigned long long *doob = (unsigned long long *)p->bOob.p;
+  CU(cudaMemsetAsync(doob, 0, sizeof(unsigned long long), st));
+  if (p->K == 0) {  // every term out of bounds
+    CU(cudaMemsetAsync(d_idx, 0xff, (size_t)p->No * terms * sizeof(int64_t), st));
+    if (oob_count) *oob_count = p->No * terms;
+    return 0;
+  }
+  L.idx = d_idx;
+  L.oob = doob;
+  const int64_t chunk = std::max<int64_t>(int64_t(1) << 16, ((int64_t(1) << 33) / terms + 255) / 256 * 256);
+  for (int64_t s0 = 0; s0 < p->No; s0 += chunk) {
+    if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
+    L.no0 = s0;
+    L.no1 = std::min(p->No, s0 + chunk);
+    cudaError_t e = f32 ? launch_plain_f32(L, st) : launch_plain_f64(L, st);
+    if (e != cudaSuccess) return cuda_fail(e, "DAS index kernel launch");
+    p->launches++;
+  }
+  if (oob_count) {
+    unsigned long long h = 0;
+    CU(cudaMemcpyAsync(&h, doob, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    *oob_count = (int64_t)h;
+  }
+  return 0;
+}
+
 int dream_das_run_device(dream_das_plan *p, const void *dY, const void *dRo, const void *dGt, const void *dGr,
                          double dt, int delay_type, const void *ddelay, double cp, void *dIm, int err_level,
                          int64_t *oob_count, void *stream) {

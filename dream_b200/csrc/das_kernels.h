@@ -41,6 +41,7 @@ struct PlainLaunch {
   unsigned long long *oob;
   int64_t ny;               // elements in Y
   unsigned long long *bad;  // gather index violations (bounds-checked builds)
+  int64_t *idx;             // non-NULL: write the sample indices instead of the image
 };
 
 cudaError_t launch_plain_f64(const PlainLaunch &L, cudaStream_t st);

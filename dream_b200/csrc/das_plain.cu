@@ -41,6 +41,7 @@ struct PlainParams {
   unsigned long long *oob;
   int64_t ny;               // elements in Y (bounds-checked builds)
   unsigned long long *bad;  // gather index violations (bounds-checked builds)
+  int64_t *idx;             // index mode: idx[col * No + no] = sample index or -1
   int bigk;  // K >= 2^22 (FP32): use the conversion unit for truncation
   // uniform grids
   T tri[15];
@@ -82,7 +83,9 @@ __device__ __forceinline__ T load_y(const PlainParams<T> &P, const T *ycol, int6
 #endif
 }
 
-template <class T, int M, bool UNI, bool TAB, bool BIGK>
+// IDX: instead of gathering and summing, write every term's sample index
+// (the one the gather would read; -1 for an out-of-bounds term) to P.idx.
+template <class T, int M, bool UNI, bool TAB, bool BIGK, bool IDX = false>
 __global__ void __launch_bounds__(256) das_plain_kernel(const PlainParams<T> P) {
   using A = Ar<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -196,7 +199,11 @@ __global__ void __launch_bounds__(256) das_plain_kernel(const PlainParams<T> P) 
       T t = A::add(leg_tx(n), delay_ms);
       T tdp = A::mul((T)2, t);  // exact doubling, as 2.0*t_tr
       T p = A::mul(tdp, P.Fs);
-      if (p > (T)-1 && p < P.Kf) {
+      if constexpr (IDX) {
+        const bool v = p > (T)-1 && p < P.Kf;
+        if (active) P.idx[(int64_t)n * P.No + no] = v ? (int64_t)to_index<T, BIGK>(p) : -1;
+        oob += v ? 0 : 1;
+      } else if (p > (T)-1 && p < P.Kf) {
         im = A::add(im, load_y(P, ycol, to_index<T, BIGK>(p)));
       } else {
         oob++;
@@ -237,7 +244,12 @@ __global__ void __launch_bounds__(256) das_plain_kernel(const PlainParams<T> P) 
           T li = TAB ? tab[(i + u) * bd + tid] : inner_leg(i + u);
           T p = A::mul(A::add(lo, li), P.Fs);
           v[u] = p > (T)-1 && p < P.Kf;
-          y[u] = v[u] ? load_y(P, ycol, (int64_t)u * P.K + to_index<T, BIGK>(p)) : (T)0;
+          if constexpr (IDX) {
+            if (active) P.idx[((int64_t)o * n_in + i + u) * P.No + no] = v[u] ? (int64_t)to_index<T, BIGK>(p) : -1;
+            y[u] = (T)0;
+          } else {
+            y[u] = v[u] ? load_y(P, ycol, (int64_t)u * P.K + to_index<T, BIGK>(p)) : (T)0;
+          }
         }
 #pragma unroll
         for (int u = 0; u < UNROLL; u++) {
@@ -249,7 +261,11 @@ __global__ void __launch_bounds__(256) das_plain_kernel(const PlainParams<T> P) 
       for (; i < n_in; i++) {
         T li = TAB ? tab[i * bd + tid] : inner_leg(i);
         T p = A::mul(A::add(lo, li), P.Fs);
-        if (p > (T)-1 && p < P.Kf) {
+        if constexpr (IDX) {
+          const bool v = p > (T)-1 && p < P.Kf;
+          if (active) P.idx[((int64_t)o * n_in + i) * P.No + no] = v ? (int64_t)to_index<T, BIGK>(p) : -1;
+          oob += v ? 0 : 1;
+        } else if (p > (T)-1 && p < P.Kf) {
           im = A::add(im, load_y(P, ycol, to_index<T, BIGK>(p)));
         } else {
           oob++;
@@ -258,7 +274,7 @@ __global__ void __launch_bounds__(256) das_plain_kernel(const PlainParams<T> P) 
       }
     }
   }
-  if (active) P.Im[no] = im;
+  if (!IDX && active) P.Im[no] = im;
   add_count(P.oob, active ? oob : 0u);
 }
 
@@ -266,10 +282,10 @@ __global__ void __launch_bounds__(256) das_plain_kernel(const PlainParams<T> P) 
 // launcher
 // ---------------------------------------------------------------------------
 
-template <class T, int M, bool UNI, bool TAB>
+template <class T, int M, bool UNI, bool TAB, bool IDX = false>
 static cudaError_t launch_one(const PlainParams<T> &P, int bd, size_t smem, cudaStream_t st) {
-  auto kern = (sizeof(T) == 4 && P.bigk) ? das_plain_kernel<T, M, UNI, TAB, true>
-                                         : das_plain_kernel<T, M, UNI, TAB, false>;
+  auto kern = (sizeof(T) == 4 && P.bigk) ? das_plain_kernel<T, M, UNI, TAB, true, IDX>
+                                         : das_plain_kernel<T, M, UNI, TAB, false, IDX>;
   cudaError_t e = ensure_smem(kern, smem);
   if (e != cudaSuccess) return e;
   int64_t grid = (P.no1 - P.no0 + bd - 1) / bd;
@@ -277,7 +293,7 @@ static cudaError_t launch_one(const PlainParams<T> &P, int bd, size_t smem, cuda
   return cudaGetLastError();
 }
 
-template <class T, bool UNI>
+template <class T, bool UNI, bool IDX = false>
 static cudaError_t launch_method(int method, const PlainParams<T> &P, cudaStream_t st) {
   const int n_in = (method == SAFT) ? 0 : (method == RCA_ROWTX ? P.Nt : P.Nr);
   // Largest block whose per-thread inner-leg table fits in 64 KB (three
@@ -288,15 +304,16 @@ static cudaError_t launch_method(int method, const PlainParams<T> &P, cudaStream
   if (!tab) bd = 128;
   size_t smem = tab ? (size_t)n_in * bd * sizeof(T) : 0;
   switch (method) {
-    case SAFT: return launch_one<T, SAFT, UNI, false>(P, 256, 0, st);
+    case SAFT: return launch_one<T, SAFT, UNI, false, IDX>(P, 256, 0, st);
     case TFM:
-      return tab ? launch_one<T, TFM, UNI, true>(P, bd, smem, st) : launch_one<T, TFM, UNI, false>(P, bd, 0, st);
+      return tab ? launch_one<T, TFM, UNI, true, IDX>(P, bd, smem, st)
+                 : launch_one<T, TFM, UNI, false, IDX>(P, bd, 0, st);
     case RCA_COLTX:
-      return tab ? launch_one<T, RCA_COLTX, UNI, true>(P, bd, smem, st)
-                 : launch_one<T, RCA_COLTX, UNI, false>(P, bd, 0, st);
+      return tab ? launch_one<T, RCA_COLTX, UNI, true, IDX>(P, bd, smem, st)
+                 : launch_one<T, RCA_COLTX, UNI, false, IDX>(P, bd, 0, st);
     case RCA_ROWTX:
-      return tab ? launch_one<T, RCA_ROWTX, UNI, true>(P, bd, smem, st)
-                 : launch_one<T, RCA_ROWTX, UNI, false>(P, bd, 0, st);
+      return tab ? launch_one<T, RCA_ROWTX, UNI, true, IDX>(P, bd, smem, st)
+                 : launch_one<T, RCA_ROWTX, UNI, false, IDX>(P, bd, 0, st);
   }
   return cudaErrorInvalidValue;
 }
@@ -320,6 +337,7 @@ static PlainParams<T> make_params(const PlainLaunch &L) {
   P.oob = L.oob;
   P.ny = L.ny;
   P.bad = L.bad;
+  P.idx = L.idx;
   P.bigk = L.K >= (int64_t(1) << 22);
   P.Nx = L.Nx;
   P.Ny = L.Ny;
@@ -334,6 +352,9 @@ cudaError_t launch_plain_f64(const PlainLaunch &L, cudaStream_t st) {
   P.delay_ms = L.c64.delay_ms;
   P.Kf = (double)L.K;
   for (int i = 0; i < 15; i++) P.tri[i] = L.tri64[i];
+  if (L.idx)
+    return L.uni ? launch_method<double, true, true>(L.method, P, st)
+                 : launch_method<double, false, true>(L.method, P, st);
   return L.uni ? launch_method<double, true>(L.method, P, st) : launch_method<double, false>(L.method, P, st);
 }
 
@@ -344,6 +365,9 @@ cudaError_t launch_plain_f32(const PlainLaunch &L, cudaStream_t st) {
   P.delay_ms = L.c32.delay_ms;
   P.Kf = (float)L.K;
   for (int i = 0; i < 15; i++) P.tri[i] = L.tri32[i];
+  if (L.idx)
+    return L.uni ? launch_method<float, true, true>(L.method, P, st)
+                 : launch_method<float, false, true>(L.method, P, st);
   return L.uni ? launch_method<float, true>(L.method, P, st) : launch_method<float, false>(L.method, P, st);
 }
 

@@ -167,6 +167,23 @@ int dream_das_uni_run_device(dream_das_plan *plan, const void *dY, const double 
                              double delay, double cp, void *dIm, int err_level,
                              int64_t *oob_count, void *stream);
 
+/*
+ * The sample index of every term: d_idx[c * No + n] = k(n, c) in [0, K), the
+ * sample of A-scan column c that das() adds for image point n, or -1 when the
+ * term is out of bounds (DAS<T>::das's per-term truncation and bounds test,
+ * extra_src/das.cc:306-626). This is the sparse DAS matrix: row n has the
+ * entry 1 (or the column's weight) at column c * K + k(n, c), and summing a
+ * row in column order gives das()'s image bit for bit (the reference builds
+ * the matrix densely in examples/model_based_example.m:381-456). F32 plans
+ * give das_f's indices; F64, F32_STORE and BF16_STORE plans das's FP64 ones.
+ * Ro, Gt, Gr and the delay are in the plan's geometry precision (FP32 for F32
+ * plans, FP64 otherwise). d_idx holds terms x No int64 values; oob_count
+ * (optional; synchronises the stream) receives the out-of-bounds terms.
+ */
+int dream_das_indices_device(dream_das_plan *plan, const void *dRo, const void *dGt, const void *dGr, double dt,
+                             int delay_type, const void *ddelay, double cp, int64_t *d_idx,
+                             int64_t *oob_count, void *stream);
+
 /* Number of kernels this plan has launched since it was created. */
 int64_t dream_das_plan_launch_count(const dream_das_plan *plan);
 
