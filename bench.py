@@ -425,6 +425,55 @@ def conv_bench(dev, cpu_sample: bool = True):
     return out
 
 
+def sir_bench(dev, cpu_sample: bool = True):
+    """Spatial impulse responses of a rectangular element (dreamrect, no
+    attenuation) on the GPU, bit-identical to the reference: (1) the reference
+    TFM test's element and field line (python/tests/test_das_tfm.py:25-96:
+    0.4 x 50 mm element, 0.05 mm discretisation, 101 points at z = 10 mm,
+    nt = 2000); (2) a field of 128 x 128 points (x in [-10, 10], z in [1, 30]
+    mm) of a 2 x 2 mm element at 0.01 mm discretisation, dt = 0.01 us,
+    nt = 4000: 6.6e8 surface-element terms. Device-resident points; the
+    unit is one surface-element term."""
+    import torch
+    from dream_b200.dreamrect import dreamrect
+    out = {}
+
+    def timed(fn, n=3):
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(n):
+            fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) * 1e3 / n
+
+    x = np.linspace(-25.0, 25.0, 101)
+    line = np.stack([x, np.zeros_like(x), np.full_like(x, 10.0)], 1)
+    X, Z = np.meshgrid(np.linspace(-10, 10, 128), np.linspace(1, 30, 128))
+    field = np.stack([X.ravel(order="F"), np.zeros(X.size), Z.ravel(order="F")], 1)
+    cfgs = {"tfm_test_line": (line, [0.4, 50.0], [0.05, 0.05, 0.02, 2000], [1.0, 1500.0, 0.0], 8 * 1000),
+            "field_128x128": (field, [2.0, 2.0], [0.01, 0.01, 0.01, 4000], [1.0, 1500.0, 0.0], 200 * 200)}
+    for name, (Ro, g, sp, mp, n_el) in cfgs.items():
+        Rd = torch.from_numpy(np.ascontiguousarray(Ro.T)).to(dev).t()
+        ms = timed(lambda: dreamrect(Rd, g, sp, 0.0, mp, "ignore"))
+        terms = Ro.shape[0] * n_el
+        out[name] = {"points": Ro.shape[0], "elements_per_point": n_el, "nt": sp[3], "ms": ms,
+                     "gterms_s": terms / ms / 1e6}
+    if cpu_sample:
+        from oracle import oracle
+        Ro, g, sp, mp, n_el = cfgs["field_128x128"]
+        sample = Ro[:: Ro.shape[0] // 8][:8]
+        t0 = time.perf_counter()
+        R = oracle.reference_rect(sample, g[0], g[1], sp[0], sp[1], sp[2], sp[3], 0.0, mp[0], mp[1])
+        dt_cpu = time.perf_counter() - t0
+        if R is not None:
+            out["cpu_baseline"] = {"gterms_s": 8 * n_el / dt_cpu / 1e9, "cores": 1, "kind": "reference",
+                                   "sample": "8 points of field_128x128 through the reference's "
+                                             "opencl/dreamrect.cl compiled as C (oracle/_ref)"}
+    out["note"] = "wall time around the call (includes the status read-back); unit = one surface-element term"
+    return out
+
+
 def batch_bench(dev, steps: int = 10, n_frames: int = 48):
     """48 uneven TFM frames (elements from {16,32,64,128}, K ~ U{1024..4096},
     cp ~ U[1450,1550], grids 64^2..512^2), FP32, one persistent launch captured
@@ -458,7 +507,8 @@ def batch_bench(dev, steps: int = 10, n_frames: int = 48):
 
 
 CASES = ("fast_f32", "fast_bf16", "plain_f64", "plain_f32", "saft_fast", "saft_plain_f64", "uni_f32",
-         "batch", "op_gather", "op_adjoint", "op_wgrad", "op_backward", "rca_bf16", "rca_f32", "conv_dp", "conv_pulse")
+         "batch", "op_gather", "op_adjoint", "op_wgrad", "op_backward", "rca_bf16", "rca_f32", "conv_dp", "conv_pulse",
+         "sir_field")
 
 
 def run_case(name: str, repeat: int = 3):
@@ -473,6 +523,7 @@ def run_case(name: str, repeat: int = 3):
       rca_bf16 / rca_f32                             RCA 128x128 row-tx, K=4096, 128x128x256 grid
       conv_dp / conv_pulse                           fftconv_p of the TFM synthesis: 2000x101 SIRs with a
                                                      2000-sample column / 3999x101 with the 150-sample pulse
+      sir_field                                      dreamrect, 2x2 mm element at 0.01 mm, 32x32 points, nt 4000
     Prints one JSON line with the mean wall time per call (not a bench value)."""
     import torch
     from dream_b200 import das, das_f, synth
@@ -537,6 +588,12 @@ def run_case(name: str, repeat: int = 3):
         A = torch.from_numpy(np.ascontiguousarray(rng.normal(size=(101, M)))).to(dev).t()
         B = torch.from_numpy(rng.normal(size=Lp)).to(dev)
         fn = lambda: fftconv_p(A, B)
+    elif name == "sir_field":
+        from dream_b200.dreamrect import dreamrect
+        X, Z = np.meshgrid(np.linspace(-10, 10, 32), np.linspace(1, 30, 32))
+        Ro = np.stack([X.ravel(order="F"), np.zeros(X.size), Z.ravel(order="F")], 1)
+        Rd = torch.from_numpy(np.ascontiguousarray(Ro.T)).to(dev).t()
+        fn = lambda: dreamrect(Rd, [2.0, 2.0], [0.01, 0.01, 0.01, 4000], 0.0, [1.0, 1500.0, 0.0], "ignore")
     else:
         raise SystemExit(f"unknown case {name!r}; one of {', '.join(CASES)}")
     fn()
@@ -702,6 +759,7 @@ def main():
     batched = batch_bench(dev)
     rca = rca_bench(dev)
     conv = conv_bench(dev, cpu_sample=(rank == 0 and not args.no_cpu_baseline))
+    sir = sir_bench(dev, cpu_sample=(rank == 0 and not args.no_cpu_baseline))
     peaks = measure_peaks(dev)
 
     if world > 1:
@@ -735,6 +793,7 @@ def main():
         "batched": batched,
         "rca": rca,
         "conv_fmc": conv,
+        "sir_dreamrect": sir,
         "autotuned": {("bf16_store" if k == _lib.PREC_BF16_STORE else "f32_store"): v for k, v in tuned.items()},
         "roofline_l2": l2_roofline(sums, step_ms, peaks),
         "peaks": peaks,

@@ -1,8 +1,12 @@
 #!/usr/bin/env bash
 # Builds the reference DREAM delay-and-sum CPU implementation, unmodified, from
 # its own sources into oracle/_ref/ as the pybind11 modules `das` (FP64) and
-# `das_f` (FP32). These modules are test infrastructure: they pin the oracle
-# and serve as the timed CPU baseline. Nothing on the product path loads them.
+# `das_f` (FP32), and the reference's rectangular-transducer SIR kernel
+# (opencl/dreamrect.cl, OpenCL C that compiles as plain C through
+# oracle/cl_shim.h) as libref_dreamrect.so. These are test infrastructure: they
+# pin the oracles and serve as CPU baselines. Nothing on the product path
+# loads them. (The reference's CPU dreamrect.cc needs FFTW for its
+# attenuation path and cannot be built here.)
 #
 # Sources compiled (paths inside the reference tree):
 #   python/src/py_das.cc  extra_src/das.cc  src/affinity.cc  src/dream_error.cc
@@ -28,4 +32,6 @@ FLAGS=(-O3 -ffp-contract=off -std=c++14 -shared -fPIC -DDREAM_PYTHON
        -I "$REF/include" -I "$REF/python/include" -I "$PYINC" -I "$PBINC" -lpthread)
 g++ "${FLAGS[@]}" "${SRCS[@]}" -o "$OUT/das$EXT"
 g++ "${FLAGS[@]}" -DUSE_FLOAT "${SRCS[@]}" -o "$OUT/das_f$EXT"
-echo "build_ref: built $OUT/das$EXT and $OUT/das_f$EXT"
+gcc -O2 -ffp-contract=off -std=gnu99 -shared -fPIC -include "$HERE/cl_shim.h" -x c "$REF/opencl/dreamrect.cl" \
+    -x none "$HERE/cl_dreamrect_driver.c" -o "$OUT/libref_dreamrect.so" -lm
+echo "build_ref: built $OUT/das$EXT, $OUT/das_f$EXT and $OUT/libref_dreamrect.so"

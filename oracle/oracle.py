@@ -30,7 +30,7 @@ _lib = None
 
 def build() -> str:
     """Compiles das_oracle.c and conv_oracle.c with gcc (make) if the shared object is stale."""
-    srcs = [os.path.join(HERE, f) for f in ("das_oracle.c", "conv_oracle.c")]
+    srcs = [os.path.join(HERE, f) for f in ("das_oracle.c", "conv_oracle.c", "rect_oracle.c")]
     if (not os.path.exists(LIB_PATH)) or os.path.getmtime(LIB_PATH) < max(os.path.getmtime(f) for f in srcs):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB_PATH
@@ -58,6 +58,8 @@ def lib():
         L.dream_oracle_das_wgrad_f64.argtypes = [vp, i64, i64, i64, vp, vp, vp]
         L.dream_oracle_conv_p.argtypes = [vp, i64, i64, vp, i64, i64, vp, i32]
         L.dream_oracle_conv_p.restype = None
+        L.dream_oracle_rect.argtypes = [vp, i64, f64, f64, f64, f64, f64, i64, i32, vp, f64, f64, i32, vp, vp]
+        L.dream_oracle_rect.restype = i32
         _lib = L
     return _lib
 
@@ -200,3 +202,31 @@ def conv_p(A, B, Y=None, mode="="):
     p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
     lib().dream_oracle_conv_p(p(A), A_M, A_N, p(B), B_M, B_N, p(Y), CONV_MODES[mode])
     return Y
+
+
+def rect(Ro, a, b, dx, dy, dt, nt, delay, v, cp, err_level="ignore"):
+    """Oracle dreamrect (rect_oracle.c, no attenuation): returns
+    ``(H, status, oob)``, H nt x No FP64 column-major."""
+    Ro = np.asfortranarray(np.asarray(Ro, dtype=np.float64))
+    delay = np.ascontiguousarray(np.asarray(delay, dtype=np.float64).reshape(-1))
+    No = Ro.shape[0]
+    H = np.zeros((int(nt), No), dtype=np.float64, order="F")
+    oob = ctypes.c_int64(0)
+    st = lib().dream_oracle_rect(_p(Ro), No, a, b, dx, dy, dt, int(nt), int(delay.size > 1), _p(delay), v, cp,
+                                 ERR_LEVELS[err_level], _p(H), ctypes.byref(oob))
+    return H, st, oob.value
+
+
+def reference_rect(Ro, a, b, dx, dy, dt, nt, delay, v, cp):
+    """The reference's OpenCL dreamrect kernel compiled as C (oracle/_ref,
+    built by build_ref.sh from /root/reference), or None when absent."""
+    path = os.path.join(REF_DIR, "libref_dreamrect.so")
+    if not os.path.exists(path):
+        return None
+    L = ctypes.CDLL(path)
+    L.dream_ref_dreamrect.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 5 + \
+        [ctypes.c_int] + [ctypes.c_double] * 3 + [ctypes.c_void_p]
+    Ro = np.asfortranarray(np.asarray(Ro, dtype=np.float64))
+    H = np.zeros((int(nt), Ro.shape[0]), dtype=np.float64, order="F")
+    L.dream_ref_dreamrect(_p(Ro), Ro.shape[0], a, b, dx, dy, dt, int(nt), float(delay), v, cp, _p(H))
+    return H
