@@ -110,7 +110,7 @@ struct dream_das_plan {
   int64_t l2_block = 0;        // A-scan bytes per inner-element pass (0: automatic, < 0: never split)
   // host-pointer runs of FP32/BF16-storage plans: A-scan upload stream
   cudaStream_t copy_stream = nullptr;
-  cudaEvent_t chunk_ev[8] = {nullptr};
+  cudaEvent_t chunk_ev[16] = {nullptr};  // [0, 15): upload chunks, [15]: fence on the previous call
   // geometry-bound operator
   bool bound = false;
   FastParams geo{};
@@ -318,7 +318,8 @@ void fast_tile(const dream_das_plan *p, int n_out, int &tf, int &ts, int &wf) {
 
 int launch_fast_plan(dream_das_plan *p, const void *dY, const void *dRo, const void *dGt, const void *dGr,
                      double dt, int delay_type, const void *ddelay, double cp, const float *dW, float *dIm,
-                     unsigned long long *doob, cudaStream_t st, int in_lo = 0, int in_hi = 0, int accumulate = 0) {
+                     unsigned long long *doob, cudaStream_t st, int in_lo = 0, int in_hi = 0, int accumulate = 0,
+                     int jc = 0) {
   if (delay_type != DREAM_DELAY_SINGLE && delay_type != DREAM_DELAY_MULTIPLE)
     return fail(DREAM_ERR_ARGUMENT, "unknown delay type");
   if (ddelay == nullptr) return fail(DREAM_ERR_ARGUMENT, "delay pointer is NULL");
@@ -372,7 +373,7 @@ int launch_fast_plan(dream_das_plan *p, const void *dY, const void *dRo, const v
   }
   const int n_out = (method == DREAM_DAS_RCA_ROWTX) ? F.Nr : F.Nt;
   fast_tile(p, n_out, F.tile_f, F.tile_s, F.wf);
-  F.jc = p->jc ? p->jc : 16;
+  F.jc = jc ? jc : (p->jc ? p->jc : 16);
   if (p->n_fast > 0) {
     F.n_fast = p->n_fast;
     F.n_slow = p->No / p->n_fast;
@@ -988,6 +989,23 @@ int dream_das_run_device_async(dream_das_plan *p, const void *dY, const void *dR
   return run_device_impl(p, dY, dRo, dGt, dGr, dt, delay_type, ddelay, cp, dIm, d_oob, st);
 }
 
+// Inner-element boundaries of the pipelined upload: UPLOAD_CHUNKS ranges on
+// multiples of 8 (at most 15). Every chunk's kernel recomputes the image
+// points' outer legs, so more, shorter chunks cost more than they save at the
+// ends of the pipeline: on the 64x64-element TFM frame from pinned memory,
+// 4 chunks of 16 take 1.50 ms, 8 of 8 take 1.94 ms and 8/16/16/16/8 1.55 ms.
+static std::vector<int> upload_chunks(int n_in) {
+  constexpr int UPLOAD_CHUNKS = 4;
+  const int n = std::max(1, std::min({UPLOAD_CHUNKS, 15, (n_in + 7) / 8}));
+  std::vector<int> cuts{0};
+  for (int c = 1; c < n; c++) {
+    const int b = std::min(n_in, (c * n_in / n + 7) / 8 * 8);
+    if (b > cuts.back()) cuts.push_back(b);
+  }
+  if (n_in > cuts.back()) cuts.push_back(n_in);
+  return cuts;
+}
+
 int dream_das_run(dream_das_plan *p, const void *Y, const void *Ro, const void *Gt, const void *Gr, double dt,
                   int delay_type, const void *delay, double cp, void *Im, int err_level, int64_t *oob_count) {
   if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
@@ -1031,18 +1049,15 @@ int dream_das_run(dream_das_plan *p, const void *Y, const void *Ro, const void *
       if (ev == nullptr) CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     int check = 0;
     if (method >= DREAM_DAS_RCA_COLTX && (check = check_rca_edges(p->Nt, p->Nr))) return check;
-    // chunk boundaries on multiples of 16 inner elements (the register chunk)
-    const int nch = std::max(1, std::min(4, (n_in + 15) / 16));
+    const std::vector<int> cuts = upload_chunks(n_in);
     unsigned long long *doob = (unsigned long long *)p->bOob.p;
     CU(cudaMemsetAsync(doob, 0, sizeof(unsigned long long), st));
     // the copy stream must not overwrite A-scans a previous call still reads
-    CU(cudaEventRecord(p->chunk_ev[7], st));
-    CU(cudaStreamWaitEvent(p->copy_stream, p->chunk_ev[7], 0));
+    CU(cudaEventRecord(p->chunk_ev[15], st));
+    CU(cudaStreamWaitEvent(p->copy_stream, p->chunk_ev[15], 0));
     const size_t pitch = (size_t)n_in * p->K * 4;
-    for (int c = 0; c < nch; c++) {
-      const int lo = std::min(n_in, ((c * n_in / nch) + 15) / 16 * 16);
-      const int hi = (c == nch - 1) ? n_in : std::min(n_in, (((c + 1) * n_in / nch) + 15) / 16 * 16);
-      if (hi <= lo) continue;
+    for (size_t c = 0; c + 1 < cuts.size(); c++) {
+      const int lo = cuts[c], hi = cuts[c + 1];
       const size_t off = (size_t)lo * p->K * 4, width = (size_t)(hi - lo) * p->K * 4;
       CU(cudaMemcpy2DAsync((char *)p->bY.p + off, pitch, (const char *)Y + off, pitch, width, (size_t)n_out,
                            cudaMemcpyHostToDevice, p->copy_stream));
@@ -1053,8 +1068,10 @@ int dream_das_run(dream_das_plan *p, const void *Y, const void *Ro, const void *
       }
       CU(cudaEventRecord(p->chunk_ev[c], p->copy_stream));
       CU(cudaStreamWaitEvent(st, p->chunk_ev[c], 0));
+      // a register chunk that divides the range keeps every chunk full
+      const int jc = ((hi - lo) % 16 == 0) ? 16 : (((hi - lo) % 8 == 0) ? 8 : 0);
       r = launch_fast_plan(p, bf16 ? p->bY16.p : p->bY.p, p->bRo.p, p->bGt.p, p->bGr.p, dt, delay_type, p->bDelay.p,
-                           cp, nullptr, (float *)p->bIm.p, doob, st, lo, hi, c > 0 ? 1 : 0);
+                           cp, nullptr, (float *)p->bIm.p, doob, st, lo, hi, c > 0 ? 1 : 0, jc);
       if (r) return r;
     }
     CU(cudaMemcpyAsync(Im, p->bIm.p, (size_t)p->No * is, cudaMemcpyDeviceToHost, st));
