@@ -427,18 +427,19 @@ def conv_bench(dev, cpu_sample: bool = True):
 
 def sir_bench(dev, cpu_sample: bool = True):
     """Spatial impulse responses of a rectangular element (dreamrect, no
-    attenuation) on the GPU, bit-identical to the reference: (1) the reference
-    TFM test's element and field line (python/tests/test_das_tfm.py:25-96:
-    0.4 x 50 mm element, 0.05 mm discretisation, 101 points at z = 10 mm,
-    nt = 2000); (2) a field of 128 x 128 points (x in [-10, 10], z in [1, 30]
-    mm) of a 2 x 2 mm element at 0.01 mm discretisation, dt = 0.01 us,
-    nt = 4000: 6.6e8 surface-element terms. Device-resident points; the
-    unit is one surface-element term."""
+    attenuation) on the GPU, bit-identical to the reference: (1) the
+    reference's own dreamrect benchmark (python/tests/bench_dreamrect.py: a
+    10 x 15 mm element at 0.05 mm = 60000 surface elements, a 61 x 61 x 256
+    field of 952576 points, dt = 0.25 us, nt = 300, cp = 1000 m/s: 5.7e10
+    surface-element terms, 2.3 GB of SIRs); (2) the reference TFM test's
+    element and field line (python/tests/test_das_tfm.py:25-96: 0.4 x 50 mm
+    at 0.05 mm, 101 points at z = 10 mm, nt = 2000). Device-resident points;
+    the unit is one surface-element term."""
     import torch
     from dream_b200.dreamrect import dreamrect
     out = {}
 
-    def timed(fn, n=3):
+    def timed(fn, n):
         fn()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -449,27 +450,30 @@ def sir_bench(dev, cpu_sample: bool = True):
 
     x = np.linspace(-25.0, 25.0, 101)
     line = np.stack([x, np.zeros_like(x), np.full_like(x, 10.0)], 1)
-    X, Z = np.meshgrid(np.linspace(-10, 10, 128), np.linspace(1, 30, 128))
-    field = np.stack([X.ravel(order="F"), np.zeros(X.size), Z.ravel(order="F")], 1)
-    cfgs = {"tfm_test_line": (line, [0.4, 50.0], [0.05, 0.05, 0.02, 2000], [1.0, 1500.0, 0.0], 8 * 1000),
-            "field_128x128": (field, [2.0, 2.0], [0.01, 0.01, 0.01, 4000], [1.0, 1500.0, 0.0], 200 * 200)}
-    for name, (Ro, g, sp, mp, n_el) in cfgs.items():
+    X, Yg, Z = np.meshgrid(np.linspace(-15, 15, 61), np.linspace(-15, 15, 61), np.linspace(1.25, 65, 256),
+                           indexing="ij")
+    field = np.stack([X.ravel(order="F"), Yg.ravel(order="F"), Z.ravel(order="F")], 1)
+    cfgs = {"bench_dreamrect": (field, [10.0, 15.0], [0.05, 0.05, 0.25, 300], [1.0, 1000.0, 0.0], 200 * 300, 2),
+            "tfm_test_line": (line, [0.4, 50.0], [0.05, 0.05, 0.02, 2000], [1.0, 1500.0, 0.0], 8 * 1000, 3)}
+    for name, (Ro, g, sp, mp, n_el, reps) in cfgs.items():
         Rd = torch.from_numpy(np.ascontiguousarray(Ro.T)).to(dev).t()
-        ms = timed(lambda: dreamrect(Rd, g, sp, 0.0, mp, "ignore"))
+        ms = timed(lambda: dreamrect(Rd, g, sp, 0.0, mp, "stop"), reps)
         terms = Ro.shape[0] * n_el
         out[name] = {"points": Ro.shape[0], "elements_per_point": n_el, "nt": sp[3], "ms": ms,
                      "gterms_s": terms / ms / 1e6}
+        del Rd
+        torch.cuda.empty_cache()
     if cpu_sample:
         from oracle import oracle
-        Ro, g, sp, mp, n_el = cfgs["field_128x128"]
-        sample = Ro[:: Ro.shape[0] // 8][:8]
+        Ro, g, sp, mp, n_el, _ = cfgs["bench_dreamrect"]
+        sample = Ro[:: Ro.shape[0] // 16][:16]
         t0 = time.perf_counter()
         R = oracle.reference_rect(sample, g[0], g[1], sp[0], sp[1], sp[2], sp[3], 0.0, mp[0], mp[1])
         dt_cpu = time.perf_counter() - t0
         if R is not None:
-            out["cpu_baseline"] = {"gterms_s": 8 * n_el / dt_cpu / 1e9, "cores": 1, "kind": "reference",
-                                   "sample": "8 points of field_128x128 through the reference's "
-                                             "opencl/dreamrect.cl compiled as C (oracle/_ref)"}
+            out["cpu_baseline"] = {"gterms_s": 16 * n_el / dt_cpu / 1e9, "cores": 1, "kind": "reference",
+                                   "sample": "16 points of bench_dreamrect through the reference's "
+                                             "opencl/dreamrect.cl compiled as C (oracle/_ref, one thread)"}
     out["note"] = "wall time around the call (includes the status read-back); unit = one surface-element term"
     return out
 

@@ -13,13 +13,15 @@
 //
 // Layout. One warp per observation point. The samples a point can receive
 // lie between the travel times to the nearest and the farthest point of the
-// a x b rectangle (+-2 samples); that window of its SIR sits in shared
-// memory (1024 samples per warp, 8 warps per CTA), wider ones are
+// a x b rectangle (+-2 samples), at most the travel-time difference across
+// its diagonal; that window of the SIR sits in shared memory (sized by the
+// diagonal bound, up to 8 warps per CTA), windows beyond 192 KB per CTA are
 // accumulated in the output column itself. The warp
 // takes 32 consecutive elements per step: lanes that hit the same sample are
 // grouped (__match_any_sync) and the lowest lane of each group adds the
-// group's amplitudes in lane order, so every sample receives its terms in
-// element order and the SIR equals the reference's bit for bit.
+// group's amplitudes in lane order (as many shuffle steps as the largest
+// group has members), so every sample receives its terms in element order
+// and the SIR equals the reference's bit for bit.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -37,8 +39,8 @@ namespace dream {
 namespace {
 
 constexpr double RECT_TWO_PI = 2 * 3.14159265358979323846;  // 2*M_PI as the reference evaluates it
-constexpr int RECT_WARPS = 8;   // observation points per CTA
-constexpr int RECT_WIN = 1024;  // samples of a point's SIR window held in shared memory
+constexpr int RECT_WARPS = 8;                     // observation points per CTA
+constexpr int64_t RECT_SMEM_MAX = 192 * 1024;     // shared memory for the CTA's SIR windows
 
 struct RectParams {
   const double *Ro;
@@ -47,6 +49,7 @@ struct RectParams {
   int nx, ny;
   double ds, dt, v, cp;
   double half_a, half_b;  // a/2, b/2
+  int64_t win;             // samples of a point's SIR window in shared memory (0: none)
   int64_t nt;
   const double *delay;
   int delay_multi;
@@ -61,10 +64,10 @@ __device__ __forceinline__ int64_t rect_sample(double r, double dlay, const Rect
 }
 
 __global__ void __launch_bounds__(RECT_WARPS * 32) rect_kernel(const RectParams P) {
-  extern __shared__ __align__(16) double rect_dyn[];  // [RECT_WARPS][RECT_WIN]
-  double (*rect_sm)[RECT_WIN] = reinterpret_cast<double (*)[RECT_WIN]>(rect_dyn);
+  extern __shared__ __align__(16) double rect_dyn[];  // [warps][P.win]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int64_t n = (int64_t)blockIdx.x * RECT_WARPS + warp;
+  double *win_sm = rect_dyn + (int64_t)warp * P.win;
+  const int64_t n = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
   if (n >= P.No) return;  // whole warps only: no block-wide barrier below
   const double xo = P.Ro[n], yo = P.Ro[n + P.No], zo = P.Ro[n + 2 * P.No];
   const double dlay = P.delay[P.delay_multi ? n : 0];
@@ -77,11 +80,11 @@ __global__ void __launch_bounds__(RECT_WARPS * 32) rect_kernel(const RectParams 
   const double r_lo = sqrt(ex * ex + ey * ey + zo * zo), r_hi = sqrt(fx * fx + fy * fy + zo * zo);
   const int64_t s_a = rect_sample(r_lo, dlay, P), s_b = rect_sample(r_hi, dlay, P);
   const int64_t w0 = max((int64_t)0, min(s_a, s_b) - 2), w1 = min(P.nt, max(s_a, s_b) + 3);
-  const bool in_smem = w1 - w0 <= RECT_WIN;
+  const bool in_smem = w1 - w0 <= P.win;
   // the SIR: shared-memory window (offset w0) or the output column itself
-  double *h = in_smem ? rect_sm[warp] - w0 : out;
+  double *h = in_smem ? win_sm - w0 : out;
   if (in_smem) {
-    for (int64_t i = lane; i < RECT_WIN; i += 32) rect_sm[warp][i] = 0.0;
+    for (int64_t i = lane; i < P.win; i += 32) win_sm[i] = 0.0;
   } else {
     for (int64_t i = lane; i < P.nt; i += 32) out[i] = 0.0;
   }
@@ -112,17 +115,23 @@ __global__ void __launch_bounds__(RECT_WARPS * 32) rect_kernel(const RectParams 
     const unsigned long long key = in ? (unsigned long long)it : ~0ull - (unsigned long long)lane;
     const unsigned int group = __match_any_sync(0xffffffffu, key);
     const bool leader = in && (__ffs(group) - 1) == lane;
+    // each leader walks its group's lanes in ascending order (its own first);
+    // the warp takes as many steps as the largest group has members
+    const unsigned int steps = __reduce_max_sync(0xffffffffu, leader ? (unsigned)__popc(group) : 0u);
     double acc = leader ? h[it] : 0.0;
-#pragma unroll 4
-    for (int j = 0; j < 32; j++) {
-      const double aj = __shfl_sync(0xffffffffu, ai, j);
-      if (leader && ((group >> j) & 1u)) acc = __dadd_rn(acc, aj);
+    unsigned int rem = leader ? group : 0u;
+    for (unsigned int k = 0; k < steps; k++) {
+      const int src = rem ? __ffs(rem) - 1 : lane;
+      const bool add = rem != 0u;
+      rem &= rem - 1u;
+      const double aj = __shfl_sync(0xffffffffu, ai, src);
+      if (add) acc = __dadd_rn(acc, aj);
     }
     if (leader) h[it] = acc;
     __syncwarp();  // this step's sums are visible to the next step's leaders
   }
   if (in_smem) {
-    for (int64_t i = lane; i < P.nt; i += 32) out[i] = (i >= w0 && i < w1) ? rect_sm[warp][i - w0] : 0.0;
+    for (int64_t i = lane; i < P.nt; i += 32) out[i] = (i >= w0 && i < w1) ? win_sm[i - w0] : 0.0;
   }
   add_count(P.oob, oob);
 }
@@ -230,10 +239,22 @@ int rect_device(RectBuffers &rb, const double *dRo, int64_t No, double a, double
   if (nx == 0 || ny == 0) {  // no surface element: the SIRs are zero
     e = cudaMemsetAsync(dH, 0, (size_t)No * nt * 8, st);
   } else {
-    const unsigned grid = (unsigned)((No + RECT_WARPS - 1) / RECT_WARPS);
-    const size_t bytes = (size_t)RECT_WARPS * RECT_WIN * sizeof(double);
-    e = ensure_smem(rect_kernel, bytes);
-    if (e == cudaSuccess) rect_kernel<<<grid, RECT_WARPS * 32, bytes, st>>>(P);
+    // No point's window is wider than the travel-time difference across the
+    // rectangle's diagonal (+ the +-2 margin and rounding): size the shared
+    // windows by that bound, so short responses leave room for many warps.
+    const double span = std::sqrt(a * a + b * b) * 1000.0 / std::fabs(cp) / std::fabs(dt);
+    int64_t win = std::isfinite(span) ? std::min<int64_t>(nt, (int64_t)span + 8) : nt;
+    int warps = RECT_WARPS;
+    while (warps > 1 && (int64_t)warps * win * 8 > RECT_SMEM_MAX) warps >>= 1;
+    if ((int64_t)warps * win * 8 > RECT_SMEM_MAX) {  // very long windows: accumulate in the output columns
+      win = 0;
+      warps = RECT_WARPS;
+    }
+    P.win = win;
+    const unsigned grid = (unsigned)((No + warps - 1) / warps);
+    const size_t bytes = (size_t)warps * win * sizeof(double);
+    e = ensure_smem(rect_kernel, RECT_SMEM_MAX);
+    if (e == cudaSuccess) rect_kernel<<<grid, warps * 32, bytes, st>>>(P);
     if (e == cudaSuccess) e = cudaGetLastError();
   }
   unsigned long long h_oob = 0;
