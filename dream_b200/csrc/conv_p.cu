@@ -129,35 +129,46 @@ __global__ void __launch_bounds__(CONV_WARPS * 32) conv_p_kernel(const double *_
     // window sample q0 + s0 + t; the B samples are ys[L-1-s0-u]
     auto xsamp = [&](int64_t t) { return xs[conv_sw(q0 + t)]; };
     auto bsamp = [&](int64_t s) { return ys[std::max<int64_t>(L - 1 - s, 0)]; };  // clamped past the end, unused
-    double acc[CONV_R], cur[CONV_R], nxt[CONV_R], yv[CONV_R];
+    // A samples in three buffers (the group's, the next group's, the one after
+    // being loaded), B samples in two; six groups per loop trip make every
+    // buffer's role fixed, so nothing is copied between groups.
+    double acc[CONV_R], X0[CONV_R], X1[CONV_R], X2[CONV_R], Y0[CONV_R], Y1[CONV_R];
 #pragma unroll
     for (int r = 0; r < CONV_R; r++) {
       const int64_t k = k_cta + q0 + r;
       acc[r] = MODE == 0 ? 0.0 : (k < NY ? z[k] : 0.0);
-      cur[r] = xsamp(s_begin + r);
-      nxt[r] = xsamp(s_begin + CONV_R + r);
-      yv[r] = bsamp(s_begin + r);
+      X0[r] = xsamp(s_begin + r);
+      X1[r] = xsamp(s_begin + CONV_R + r);
+      Y0[r] = bsamp(s_begin + r);
     }
-    // Per group: the next group's samples are loaded first (they do not depend
-    // on the sums, so their latency overlaps this group's arithmetic), then
-    // R x R products and adds; only each output's FP64 add is serial.
-    for (int64_t s0 = s_begin; s0 < s_end; s0 += CONV_R) {
-      double nxt2[CONV_R], yv2[CONV_R];
+    // One group: the following group's samples are loaded first (they do not
+    // depend on the sums, so their latency overlaps this group's arithmetic),
+    // then R x R products and adds; only each output's FP64 add is serial.
+    auto group = [&](int64_t s0, const double(&cur)[CONV_R], const double(&nxt)[CONV_R], double(&load)[CONV_R],
+                     const double(&yv)[CONV_R], double(&yload)[CONV_R]) {
 #pragma unroll
       for (int u = 0; u < CONV_R; u++) {
-        nxt2[u] = xsamp(std::min<int64_t>(s0 + 2 * CONV_R + u, W - 1 - q0));
-        yv2[u] = bsamp(s0 + CONV_R + u);
+        load[u] = xsamp(std::min<int64_t>(s0 + 2 * CONV_R + u, W - 1 - q0));
+        yload[u] = bsamp(s0 + CONV_R + u);
       }
       if (s0 + CONV_R <= s_end)  // a full group: no exit test between the steps
         conv_group<MODE, true>(acc, cur, nxt, yv, s0, s_end, base + q0, M, neutral);
       else
         conv_group<MODE, false>(acc, cur, nxt, yv, s0, s_end, base + q0, M, neutral);
-#pragma unroll
-      for (int r = 0; r < CONV_R; r++) {
-        cur[r] = nxt[r];
-        nxt[r] = nxt2[r];
-        yv[r] = yv2[r];
-      }
+    };
+    for (int64_t s0 = s_begin; s0 < s_end;) {
+      group(s0, X0, X1, X2, Y0, Y1);
+      if ((s0 += CONV_R) >= s_end) break;
+      group(s0, X1, X2, X0, Y1, Y0);
+      if ((s0 += CONV_R) >= s_end) break;
+      group(s0, X2, X0, X1, Y0, Y1);
+      if ((s0 += CONV_R) >= s_end) break;
+      group(s0, X0, X1, X2, Y1, Y0);
+      if ((s0 += CONV_R) >= s_end) break;
+      group(s0, X1, X2, X0, Y0, Y1);
+      if ((s0 += CONV_R) >= s_end) break;
+      group(s0, X2, X0, X1, Y1, Y0);
+      s0 += CONV_R;
     }
 #pragma unroll
     for (int r = 0; r < CONV_R; r++) {
