@@ -527,7 +527,8 @@ def run_case(name: str, repeat: int = 3):
       rca_bf16 / rca_f32                             RCA 128x128 row-tx, K=4096, 128x128x256 grid
       conv_dp / conv_pulse                           fftconv_p of the TFM synthesis: 2000x101 SIRs with a
                                                      2000-sample column / 3999x101 with the 150-sample pulse
-      sir_field                                      dreamrect, 2x2 mm element at 0.01 mm, 32x32 points, nt 4000
+      sir_field                                      dreamrect, the reference bench_dreamrect element on a
+                                                     16x16x32 subset of its field
     Prints one JSON line with the mean wall time per call (not a bench value)."""
     import torch
     from dream_b200 import das, das_f, synth
@@ -594,10 +595,11 @@ def run_case(name: str, repeat: int = 3):
         fn = lambda: fftconv_p(A, B)
     elif name == "sir_field":
         from dream_b200.dreamrect import dreamrect
-        X, Z = np.meshgrid(np.linspace(-10, 10, 32), np.linspace(1, 30, 32))
-        Ro = np.stack([X.ravel(order="F"), np.zeros(X.size), Z.ravel(order="F")], 1)
+        X, Yg, Z = np.meshgrid(np.linspace(-15, 15, 16), np.linspace(-15, 15, 16), np.linspace(1.25, 65, 32),
+                               indexing="ij")
+        Ro = np.stack([X.ravel(order="F"), Yg.ravel(order="F"), Z.ravel(order="F")], 1)
         Rd = torch.from_numpy(np.ascontiguousarray(Ro.T)).to(dev).t()
-        fn = lambda: dreamrect(Rd, [2.0, 2.0], [0.01, 0.01, 0.01, 4000], 0.0, [1.0, 1500.0, 0.0], "ignore")
+        fn = lambda: dreamrect(Rd, [10.0, 15.0], [0.05, 0.05, 0.25, 300], 0.0, [1.0, 1000.0, 0.0], "stop")
     else:
         raise SystemExit(f"unknown case {name!r}; one of {', '.join(CASES)}")
     fn()
