@@ -93,13 +93,15 @@ __global__ void __launch_bounds__(RECT_WARPS * 32) rect_kernel(const RectParams 
   const double vds = __dmul_rn(P.v, P.ds);
   const int64_t E = (int64_t)P.nx * P.ny;
   unsigned int oob = 0;
+  // this lane's element e = iy*nx + ix, advanced by 32 per step without a division
+  int64_t iy = lane / P.nx;
+  int ix = lane - (int)(iy * P.nx);
   for (int64_t e0 = 0; e0 < E; e0 += 32) {
     const int64_t e = e0 + lane;
     bool in = false;
     int64_t it = 0;
     double ai = 0.0;
     if (e < E) {
-      const int64_t iy = e / P.nx, ix = e - iy * P.nx;
       const double rx = __dsub_rn(xo, __ldg(P.xs + ix));
       const double ry = __dsub_rn(yo, __ldg(P.ys + iy));
       const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), rz2));
@@ -129,6 +131,11 @@ __global__ void __launch_bounds__(RECT_WARPS * 32) rect_kernel(const RectParams 
     }
     if (leader) h[it] = acc;
     __syncwarp();  // this step's sums are visible to the next step's leaders
+    ix += 32;
+    while (ix >= P.nx) {  // once for rows of 32 or more elements
+      ix -= P.nx;
+      iy++;
+    }
   }
   if (in_smem) {
     for (int64_t i = lane; i < P.nt; i += 32) out[i] = (i >= w0 && i < w1) ? win_sm[i - w0] : 0.0;
