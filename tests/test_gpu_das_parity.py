@@ -198,3 +198,28 @@ def test_cancel_between_launches():
     p.set_running()
     rc = L.dream_das_run(p.handle, ptr(Y), ptr(Ro), ptr(G), ptr(G), 0.04, 0, ptr(d), 1500.0, ptr(Im), 1, None)
     assert rc >= 0
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_long_ascans_large_indices(prec):
+    """A-scans of 8M samples (dt = 1e-5 us) with indices near 6.7M: the FP32
+    kernel truncates through the conversion path for K >= 2^22. Bit-exact
+    against the oracle, plain kernels and the FP32-storage kernel."""
+    from dream_b200 import synth
+    from dream_b200.beamformer import das_mixed
+    T = np.float64 if prec == "f64" else np.float32
+    rng = np.random.default_rng(12)
+    K = 8 << 20
+    G = np.asfortranarray(np.array([[-1.0, 0.0, 0.0], [1.5, 0.0, 0.0]]))
+    Ro = synth.grid_xz(8, 8, (-3.0, 3.0), (45.0, 55.0))
+    Y = np.asfortranarray(rng.normal(size=(K, 4)).astype(T))
+    s = synth.Scene(Y, G, G.copy(order="F"), Ro, 1e-5, np.zeros((1, 1)), 1500.0, "tfm", (8, 8)).astype(T)
+    ref, st, oob = oracle.das(s.Y, s.Gt, s.Gr, s.Ro, T(s.dt), s.delay, T(s.cp), "tfm", "ignore", T)
+    assert oob == 0
+    Im = _mod(prec).das(s.Y, s.Gt, s.Gr, s.Ro, T(s.dt), s.delay, T(s.cp), "tfm", "ignore", "cuda")
+    assert np.array_equal(Im, ref)
+    if prec == "f64":  # FP32 storage with the FP64 indices: the oracle summing the stored samples
+        Ys = np.asfortranarray(s.Y.astype(np.float32).astype(np.float64))
+        ref32, _, _ = oracle.das(Ys, s.Gt, s.Gr, s.Ro, s.dt, s.delay, s.cp, "tfm", "ignore", np.float64)
+        Im32 = das_mixed(s.Y, s.Gt, s.Gr, s.Ro, s.dt, s.delay, s.cp, "tfm", "ignore", "cuda", "f32")
+        assert np.abs(Im32 - ref32).max() <= 1e-6 * np.abs(ref32).max()
