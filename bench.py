@@ -425,6 +425,26 @@ def conv_bench(dev, cpu_sample: bool = True):
     return out
 
 
+def arr_example():
+    """The reference's array example (examples/rect_arr_example.m): a 21 x 21
+    array of 0.9 x 0.9 mm elements at 1 mm pitch (0.03 mm discretisation,
+    900 surface elements each), xy focusing at 50 mm, steering -25 degrees in
+    x, the field over two 101 x 80 mm planes (x-z and y-z) at 0.5 mm (64722
+    points), a 2 mm window at 49-51 mm (dt = 0.1 us, nt = 13, cp = 1500 m/s)."""
+    x = np.arange(-10.0, 11.0)
+    gx, gy = np.meshgrid(x, x)
+    G = np.asfortranarray(np.stack([gx.ravel(order="F"), gy.ravel(order="F"), np.zeros(gx.size)], 1))
+    xs, zs = np.arange(-50.0, 50.25, 0.5), np.arange(0.0, 80.25, 0.5)
+    X, Z = np.meshgrid(xs, zs)
+    xz = np.stack([X.ravel(order="F"), np.zeros(X.size), Z.ravel(order="F")], 1)
+    yz = np.stack([np.zeros(X.size), X.ravel(order="F"), Z.ravel(order="F")], 1)
+    Ro = np.asfortranarray(np.concatenate([xz, yz]))
+    nt = int(round(2.0 * 1e3 / 1500.0 / 0.1))
+    n_el = len(np.arange(-0.45 + 0.015, 0.45, 0.03)) ** 2
+    return {"Ro": Ro, "G": G, "M": G.shape[0], "geom": [0.9, 0.9], "s_par": [0.03, 0.03, 0.1, nt],
+            "delay": (50.0 - 1.0) * 1e3 / 1500.0, "m_par": [1.0, 1500.0, 0.0], "n_el": n_el}
+
+
 def sir_bench(dev, cpu_sample: bool = True):
     """Spatial impulse responses of a rectangular element (dreamrect, no
     attenuation) on the GPU, bit-identical to the reference: (1) the
@@ -433,10 +453,11 @@ def sir_bench(dev, cpu_sample: bool = True):
     field of 952576 points, dt = 0.25 us, nt = 300, cp = 1000 m/s: 5.7e10
     surface-element terms, 2.3 GB of SIRs); (2) the reference TFM test's
     element and field line (python/tests/test_das_tfm.py:25-96: 0.4 x 50 mm
-    at 0.05 mm, 101 points at z = 10 mm, nt = 2000). Device-resident points;
-    the unit is one surface-element term."""
+    at 0.05 mm, 101 points at z = 10 mm, nt = 2000); (3) dream_arr_rect on
+    the reference's array example (arr_example). Device-resident points; the
+    unit is one surface-element term."""
     import torch
-    from dream_b200.dreamrect import dreamrect
+    from dream_b200.dreamrect import dream_arr_rect, dreamrect
     out = {}
 
     def timed(fn, n):
@@ -463,6 +484,19 @@ def sir_bench(dev, cpu_sample: bool = True):
                      "gterms_s": terms / ms / 1e6}
         del Rd
         torch.cuda.empty_cache()
+    # (3) the reference's array example (examples/rect_arr_example.m)
+    arr = arr_example()
+    Rd = torch.from_numpy(np.ascontiguousarray(arr["Ro"].T)).to(dev).t()
+    ms = timed(lambda: dream_arr_rect(Rd, arr["geom"], arr["G"], arr["s_par"], arr["delay"], arr["m_par"], "xy", 50.0,
+                                      "x", [-25.0, 0.0], "off", np.ones(arr["M"]), 1.0, "ignore"), 3)
+    terms = arr["Ro"].shape[0] * arr["M"] * arr["n_el"]
+    out["rect_arr_example"] = {"points": arr["Ro"].shape[0], "array_elements": arr["M"],
+                               "surface_elements": arr["n_el"], "nt": arr["s_par"][3], "ms": ms,
+                               "gterms_s": terms / ms / 1e6,
+                               "note": "terms the reference evaluates; array elements whose sample window misses "
+                                       "[0, nt) for a point are counted out of bounds without being evaluated"}
+    del Rd
+    torch.cuda.empty_cache()
     if cpu_sample:
         from oracle import oracle
         Ro, g, sp, mp, n_el, _ = cfgs["bench_dreamrect"]
@@ -474,6 +508,15 @@ def sir_bench(dev, cpu_sample: bool = True):
             out["cpu_baseline"] = {"gterms_s": 16 * n_el / dt_cpu / 1e9, "cores": 1, "kind": "reference",
                                    "sample": "16 points of bench_dreamrect through the reference's "
                                              "opencl/dreamrect.cl compiled as C (oracle/_ref, one thread)"}
+        sample = arr["Ro"][:: arr["Ro"].shape[0] // 512][:512]
+        t0 = time.perf_counter()
+        oracle.arr_rect(sample, arr["geom"][0], arr["geom"][1], arr["G"], arr["s_par"][0], arr["s_par"][1],
+                        arr["s_par"][2], arr["s_par"][3], arr["delay"], 1.0, 1500.0, "xy", 50.0, "x", -25.0, 0.0)
+        dt_cpu = time.perf_counter() - t0
+        out["rect_arr_example"]["cpu_baseline"] = {
+            "gterms_s": 512 * arr["M"] * arr["n_el"] / dt_cpu / 1e9, "cores": 1, "kind": "port",
+            "sample": "512 points of rect_arr_example through the oracle's dream_arr_rect (one thread; the "
+                      "reference's CPU dream_arr_rect needs FFTW and is not built here)"}
     out["note"] = "wall time around the call (includes the status read-back); unit = one surface-element term"
     return out
 

@@ -63,6 +63,10 @@ SIGNATURES = {
     "dream_conv_p_run": (_i, [_vp, _i64, _i64, _vp, _i64, _i64, _vp, _i, _i]),
     "dream_rect_run_device": (_i, [_vp, _i64, _d, _d, _d, _d, _d, _i64, _i, _vp, _d, _d, _vp, _i, _vp, _i, _vp]),
     "dream_rect_run": (_i, [_vp, _i64, _d, _d, _d, _d, _d, _i64, _i, _vp, _d, _d, _vp, _i, _vp, _i]),
+    "dream_arr_rect_run_device": (_i, [_vp, _i64, _d, _d, _d, _d, _d, _i64, _i, _vp, _d, _d, _i64, _vp, _i, _vp,
+                                       _i, _d, _d, _i, _vp, _d, _vp, _i, _vp, _i, _vp]),
+    "dream_arr_rect_run": (_i, [_vp, _i64, _d, _d, _d, _d, _d, _i64, _i, _vp, _d, _d, _i64, _vp, _i, _vp, _i, _d,
+                                _d, _i, _vp, _d, _vp, _i, _vp, _i]),
     "dream_das_get_tile": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "dream_das_weighted_run_device": (_i, [_vp, _vp, _vp, _vp, _vp, _d, _i, _vp, _d, _vp, _vp, _vp, _vp]),
     "dream_das_bind_geometry": (_i, [_vp, _vp, _vp, _vp, _d, _i, _vp, _d, _vp]),

@@ -3,7 +3,9 @@
 # its own sources into oracle/_ref/ as the pybind11 modules `das` (FP64) and
 # `das_f` (FP32), and the reference's rectangular-transducer SIR kernel
 # (opencl/dreamrect.cl, OpenCL C that compiles as plain C through
-# oracle/cl_shim.h) as libref_dreamrect.so. These are test infrastructure: they
+# oracle/cl_shim.h) as libref_dreamrect.so, and the reference's array helpers
+# (src/arr_functions.cc: focusing, steering and apodisation of array elements)
+# with oracle/ref_arr_driver.cc as libref_arr.so. These are test infrastructure: they
 # pin the oracles and serve as CPU baselines. Nothing on the product path
 # loads them. (The reference's CPU dreamrect.cc needs FFTW for its
 # attenuation path and cannot be built here.)
@@ -34,4 +36,6 @@ g++ "${FLAGS[@]}" "${SRCS[@]}" -o "$OUT/das$EXT"
 g++ "${FLAGS[@]}" -DUSE_FLOAT "${SRCS[@]}" -o "$OUT/das_f$EXT"
 gcc -O2 -ffp-contract=off -std=gnu99 -shared -fPIC -include "$HERE/cl_shim.h" -x c "$REF/opencl/dreamrect.cl" \
     -x none "$HERE/cl_dreamrect_driver.c" -o "$OUT/libref_dreamrect.so" -lm
-echo "build_ref: built $OUT/das$EXT, $OUT/das_f$EXT and $OUT/libref_dreamrect.so"
+g++ -O2 -ffp-contract=off -std=c++14 -shared -fPIC -DDREAM_PYTHON -I "$REF/include" -I "$PYINC" -I "$PBINC" \
+    "$REF/src/arr_functions.cc" "$HERE/ref_arr_driver.cc" -o "$OUT/libref_arr.so" -lm
+echo "build_ref: built $OUT/das$EXT, $OUT/das_f$EXT, $OUT/libref_dreamrect.so and $OUT/libref_arr.so"

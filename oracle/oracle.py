@@ -60,6 +60,11 @@ def lib():
         L.dream_oracle_conv_p.restype = None
         L.dream_oracle_rect.argtypes = [vp, i64, f64, f64, f64, f64, f64, i64, i32, vp, f64, f64, i32, vp, vp]
         L.dream_oracle_rect.restype = i32
+        L.dream_oracle_arr_elements.argtypes = [vp, i64, i32, vp, i32, f64, f64, i32, vp, f64, f64, vp, vp, vp]
+        L.dream_oracle_arr_elements.restype = None
+        L.dream_oracle_arr_rect.argtypes = [vp, i64, f64, f64, f64, f64, f64, i64, i32, vp, f64, f64, i64, vp, i32,
+                                            vp, i32, f64, f64, i32, vp, f64, i32, vp, vp]
+        L.dream_oracle_arr_rect.restype = i32
         _lib = L
     return _lib
 
@@ -230,3 +235,57 @@ def reference_rect(Ro, a, b, dx, dy, dt, nt, delay, v, cp):
     H = np.zeros((int(nt), Ro.shape[0]), dtype=np.float64, order="F")
     L.dream_ref_dreamrect(_p(Ro), Ro.shape[0], a, b, dx, dy, dt, int(nt), float(delay), v, cp, _p(H))
     return H
+
+
+# Method codes of the array entries (include/dream_sir.h), by the reference's strings.
+FOC_METHODS = {"off": 0, "x": 1, "y": 2, "xy": 3, "on": 3, "x+y": 4, "ud": 5}
+STEER_METHODS = {"off": 0, "x": 1, "y": 2, "xy": 3}
+APOD_METHODS = {"off": 0, "triangle": 1, "gauss": 2, "raised": 3, "hann": 4, "hamming": 5, "simply": 6,
+                "clamped": 7, "ud": 8}
+
+
+def _arr_args(G, focal, apod):
+    G = np.asfortranarray(np.asarray(G, dtype=np.float64))
+    focal = np.ascontiguousarray(np.asarray(focal, dtype=np.float64).reshape(-1))
+    apod = None if apod is None else np.ascontiguousarray(np.asarray(apod, dtype=np.float64).reshape(-1))
+    return G, focal, apod
+
+
+def arr_elements(G, foc_met, focal, steer_met, theta, phi, apod_met, apod, apod_par, cp, reference=False):
+    """Per-element focusing delays, steering delays and weights of an array:
+    ``(foc, steer, weight)``. ``reference=True`` runs the reference's own
+    src/arr_functions.cc (oracle/_ref/libref_arr.so; None when absent)
+    instead of the restatement in rect_oracle.c."""
+    G, focal, apod = _arr_args(G, focal, apod)
+    M = G.shape[0]
+    out = [np.zeros(M) for _ in range(3)]
+    args = (_p(G), M, FOC_METHODS[foc_met], _p(focal), STEER_METHODS[steer_met], float(theta), float(phi),
+            APOD_METHODS[apod_met], _p(apod), float(apod_par), float(cp), *[_p(o) for o in out])
+    if reference:
+        path = os.path.join(REF_DIR, "libref_arr.so")
+        if not os.path.exists(path):
+            return None
+        L = ctypes.CDLL(path)
+        L.dream_ref_arr_elements.argtypes = lib().dream_oracle_arr_elements.argtypes
+        L.dream_ref_arr_elements.restype = None
+        L.dream_ref_arr_elements(*args)
+    else:
+        lib().dream_oracle_arr_elements(*args)
+    return tuple(out)
+
+
+def arr_rect(Ro, a, b, G, dx, dy, dt, nt, delay, v, cp, foc_met="off", focal=0.0, steer_met="off", theta=0.0,
+             phi=0.0, apod_met="off", apod=None, apod_par=0.0, err_level="ignore"):
+    """Oracle dream_arr_rect (rect_oracle.c, no attenuation): returns
+    ``(H, status, oob)``, H nt x No FP64 column-major."""
+    Ro = np.asfortranarray(np.asarray(Ro, dtype=np.float64))
+    G, focal, apod = _arr_args(G, focal, apod)
+    delay = np.ascontiguousarray(np.asarray(delay, dtype=np.float64).reshape(-1))
+    No = Ro.shape[0]
+    H = np.zeros((int(nt), No), dtype=np.float64, order="F")
+    oob = ctypes.c_int64(0)
+    st = lib().dream_oracle_arr_rect(_p(Ro), No, a, b, dx, dy, dt, int(nt), int(delay.size > 1), _p(delay), v, cp,
+                                     G.shape[0], _p(G), FOC_METHODS[foc_met], _p(focal), STEER_METHODS[steer_met],
+                                     float(theta), float(phi), APOD_METHODS[apod_met], _p(apod), float(apod_par),
+                                     ERR_LEVELS[err_level], _p(H), ctypes.byref(oob))
+    return H, st, oob.value
