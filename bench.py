@@ -555,7 +555,7 @@ def batch_bench(dev, steps: int = 10, n_frames: int = 48):
 
 CASES = ("fast_f32", "fast_bf16", "plain_f64", "plain_f32", "saft_fast", "saft_plain_f64", "uni_f32",
          "batch", "op_gather", "op_adjoint", "op_wgrad", "op_backward", "rca_bf16", "rca_f32", "conv_dp", "conv_pulse",
-         "sir_field")
+         "sir_field", "sir_arr")
 
 
 def run_case(name: str, repeat: int = 3):
@@ -572,6 +572,7 @@ def run_case(name: str, repeat: int = 3):
                                                      2000-sample column / 3999x101 with the 150-sample pulse
       sir_field                                      dreamrect, the reference bench_dreamrect element on a
                                                      16x16x32 subset of its field
+      sir_arr                                        dream_arr_rect, the reference's array example (arr_example)
     Prints one JSON line with the mean wall time per call (not a bench value)."""
     import torch
     from dream_b200 import das, das_f, synth
@@ -643,6 +644,12 @@ def run_case(name: str, repeat: int = 3):
         Ro = np.stack([X.ravel(order="F"), Yg.ravel(order="F"), Z.ravel(order="F")], 1)
         Rd = torch.from_numpy(np.ascontiguousarray(Ro.T)).to(dev).t()
         fn = lambda: dreamrect(Rd, [10.0, 15.0], [0.05, 0.05, 0.25, 300], 0.0, [1.0, 1000.0, 0.0], "stop")
+    elif name == "sir_arr":
+        from dream_b200.dreamrect import dream_arr_rect
+        arr = arr_example()
+        Rd = torch.from_numpy(np.ascontiguousarray(arr["Ro"].T)).to(dev).t()
+        fn = lambda: dream_arr_rect(Rd, arr["geom"], arr["G"], arr["s_par"], arr["delay"], arr["m_par"], "xy", 50.0,
+                                    "x", [-25.0, 0.0], "off", np.ones(arr["M"]), 1.0, "ignore")
     else:
         raise SystemExit(f"unknown case {name!r}; one of {', '.join(CASES)}")
     fn()

@@ -134,12 +134,15 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 
 // One warp step: lane's term (if valid) at surface element (ix, iy) of the
 // element V is added to its sample, every sample receiving its terms in lane
-// order. Lanes that hit the same sample are grouped (__match_any_sync) and
-// the lowest lane of each group adds the group's amplitudes in lane order
-// (as many shuffle steps as the largest group has members).
+// order. Lanes that hit the same sample are grouped (__match_any_sync); the
+// lowest lane of each group adds the group's amplitudes in lane order. When
+// every group is a run of consecutive lanes (the common case: along a row
+// the sample index changes monotonically on either side of the point's
+// projection) the leaders read their run from the warp's 32 staged
+// amplitudes, four per trip; otherwise they walk their member masks.
 __device__ __forceinline__ void term_step(const RectParams &P, const ElemView &V, bool valid, int ix, int iy,
-                                          int lane, int64_t w0, int64_t w1, double *h, unsigned long long &oob,
-                                          unsigned int &flags, bool last) {
+                                          int lane, int64_t w0, int64_t w1, double *h, double *stage,
+                                          unsigned long long &oob, unsigned int &flags, bool last) {
   bool in = false;
   int64_t it = 0;
   double ai = 0.0;
@@ -161,27 +164,51 @@ __device__ __forceinline__ void term_step(const RectParams &P, const ElemView &V
   // lanes adding into the same sample form a group; the others get unique keys
   const unsigned long long key = in ? (unsigned long long)it : ~0ull - (unsigned long long)lane;
   const unsigned int group = __match_any_sync(0xffffffffu, key);
-  const bool leader = in && (__ffs(group) - 1) == lane;
-  const unsigned int steps = __reduce_max_sync(0xffffffffu, leader ? (unsigned)__popc(group) : 0u);
-  double acc = leader ? h[it] : 0.0;
-  unsigned int rem = leader ? group : 0u;
-  for (unsigned int k = 0; k < steps; k++) {
-    const int src = rem ? __ffs(rem) - 1 : lane;
-    const bool add = rem != 0u;
-    rem &= rem - 1u;
-    const double aj = __shfl_sync(0xffffffffu, ai, src);
-    if (add) acc = __dadd_rn(acc, aj);
+  const int len = __popc(group);
+  const bool leader = in && (group & ((1u << lane) - 1u)) == 0u;  // lowest lane of its group
+  // a run: the group's lanes are lane .. lane + len - 1
+  const bool run = (group >> lane) == (len == 32 ? 0xffffffffu : (1u << len) - 1u);
+  if (__all_sync(0xffffffffu, !leader || run)) {
+    stage[lane] = ai;
+    __syncwarp();
+    if (leader) {
+      double acc = __dadd_rn(h[it], ai);
+      const double *q = stage + lane + 1;
+      int k = len - 1;
+      for (; k >= 4; k -= 4, q += 4) {
+        acc = __dadd_rn(acc, q[0]);
+        acc = __dadd_rn(acc, q[1]);
+        acc = __dadd_rn(acc, q[2]);
+        acc = __dadd_rn(acc, q[3]);
+      }
+      for (; k > 0; k--, q++) acc = __dadd_rn(acc, q[0]);
+      h[it] = acc;
+    }
+  } else {
+    // each leader walks its group's lanes in ascending order (its own first);
+    // the warp takes as many steps as the largest group has members
+    const unsigned int steps = __reduce_max_sync(0xffffffffu, leader ? (unsigned)len : 0u);
+    double acc = leader ? h[it] : 0.0;
+    unsigned int rem = leader ? group : 0u;
+    for (unsigned int k = 0; k < steps; k++) {
+      const int src = rem ? __ffs(rem) - 1 : lane;
+      const bool add = rem != 0u;
+      rem &= rem - 1u;
+      const double aj = __shfl_sync(0xffffffffu, ai, src);
+      if (add) acc = __dadd_rn(acc, aj);
+    }
+    if (leader) h[it] = acc;
   }
-  if (leader) h[it] = acc;
-  __syncwarp();  // this step's sums are visible to the next step's leaders
+  __syncwarp();  // this step's sums (and stage reads) complete before the next step
 }
 
 // ARR = false: dreamrect (one element at the origin, P.M == 1), ARR = true: arrays.
 template <bool ARR>
 __global__ void __launch_bounds__(RECT_WARPS * 32) rect_kernel(const RectParams P) {
-  extern __shared__ __align__(16) double rect_dyn[];  // [warps][P.win]
+  extern __shared__ __align__(16) double rect_dyn[];  // [warps][32] staged amplitudes, then [warps][P.win]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double *win_sm = rect_dyn + (int64_t)warp * P.win;
+  double *stage = rect_dyn + warp * 32;
+  double *win_sm = rect_dyn + (blockDim.x >> 5) * 32 + (int64_t)warp * P.win;
   const int64_t n = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
   if (n >= P.No) return;  // whole warps only: no block-wide barrier below
   double *out = P.H + n * P.nt;
@@ -234,7 +261,7 @@ __global__ void __launch_bounds__(RECT_WARPS * 32) rect_kernel(const RectParams 
       int iy = lane / P.nx;
       int ix = lane - iy * P.nx;
       for (int64_t e0 = 0; e0 < E; e0 += 32) {
-        term_step(P, V, e0 + lane < E, ix, iy, lane, w0, w1, h, oob, flags, true);
+        term_step(P, V, e0 + lane < E, ix, iy, lane, w0, w1, h, stage, oob, flags, true);
         ix += 32;
         while (ix >= P.nx) {  // once for rows of 32 or more elements
           ix -= P.nx;
@@ -267,7 +294,7 @@ __global__ void __launch_bounds__(RECT_WARPS * 32) rect_kernel(const RectParams 
       bool last = rest && c0 + __ffs(rest) - 1 == P.M - 1;  // this lane's element is the array's last
       if (rest) elem_view(P, c0 + __ffs(rest) - 1, n, V);
       for (int64_t g0 = 0; g0 < total; g0 += 32) {
-        term_step(P, V, g0 + lane < total, ix, iy, lane, w0, w1, h, oob, flags, last);
+        term_step(P, V, g0 + lane < total, ix, iy, lane, w0, w1, h, stage, oob, flags, last);
         // advance by 32 terms without a division (once per wrap for rows of 32 or more)
         ix += 32;
         bool next = false;
@@ -546,8 +573,8 @@ int rect_device(RectBuffers &rb, const double *dRo, int64_t No, double a, double
   for (int full = 0; full < 2 && e == cudaSuccess; full++) {
     int64_t win = full ? 0 : window_bound(el, a, b, dt, cp, nt);
     int warps = RECT_WARPS;
-    while (warps > 1 && (int64_t)warps * win * 8 > RECT_SMEM_MAX) warps >>= 1;
-    if ((int64_t)warps * win * 8 > RECT_SMEM_MAX) {  // very long windows: accumulate in the output columns
+    while (warps > 1 && (int64_t)warps * (win + 32) * 8 > RECT_SMEM_MAX) warps >>= 1;
+    if ((int64_t)warps * (win + 32) * 8 > RECT_SMEM_MAX) {  // very long windows: accumulate in the output columns
       win = 0;
       warps = RECT_WARPS;
     }
@@ -555,7 +582,7 @@ int rect_device(RectBuffers &rb, const double *dRo, int64_t No, double a, double
     P.full = full;
     const unsigned grid = (unsigned)((No + warps - 1) / warps);
     e = cudaMemsetAsync(rb.ctr, 0, sizeof(h_ctr), st);
-    if (e == cudaSuccess) kernel<<<grid, warps * 32, (size_t)warps * win * sizeof(double), st>>>(P);
+    if (e == cudaSuccess) kernel<<<grid, warps * 32, (size_t)warps * (win + 32) * sizeof(double), st>>>(P);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(h_ctr, rb.ctr, sizeof(h_ctr), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
