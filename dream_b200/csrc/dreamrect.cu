@@ -53,6 +53,10 @@ constexpr double RECT_TWO_PI = 2 * 3.14159265358979323846;  // 2*M_PI as the ref
 constexpr int RECT_WARPS = 8;                     // observation points per CTA
 constexpr int64_t RECT_SMEM_MAX = 192 * 1024;     // shared memory for the CTA's SIR windows
 constexpr double RECT_WIN_TRUST = 68719476736.0;  // 2^36: sample magnitudes whose +-2 window margin is proven
+// A sample-index estimate farther than this from a half-integer rounds like
+// the exact chain: with sample magnitudes below RECT_WIN_TRUST the two differ
+// by at most 10 * 2^-53 * 2^36 < 2^-13 samples.
+constexpr double RECT_Q_SAFE = 0.5 - 1.0 / 1024.0;
 constexpr unsigned RECT_MISS = 1u;      // a term fell in [0, nt) outside its point's window
 constexpr unsigned RECT_LAST_OOB = 2u;  // a term of the array's last element was out of bounds
 
@@ -70,6 +74,8 @@ struct RectParams {
   const ArrElem *el;      // array elements (M)
   int64_t M;
   double dt, cp;
+  double c1, inv_dt;      // 1000/cp and 1/dt, for the sample-index estimate
+  double ab;              // |a| + |b|
   double half_a, half_b;  // a/2, b/2
   int64_t win;            // samples of a point's SIR window in shared memory (0: none)
   int64_t nt;
@@ -81,9 +87,11 @@ struct RectParams {
   unsigned int *flags;            // RECT_MISS | RECT_LAST_OOB
 };
 
-// The observation point as array element m sees it.
+// The observation point as array element m sees it; `fast`: its sample
+// magnitudes are below RECT_WIN_TRUST (windows and index estimates hold).
 struct ElemView {
   double xo, yo, zo, rz2, dl, w;
+  bool fast;
 };
 
 // Point n (reloaded from global memory: kept out of the term loop's registers).
@@ -97,6 +105,8 @@ __device__ __forceinline__ void elem_view(const RectParams &P, int64_t m, int64_
   V.rz2 = __dmul_rn(V.zo, V.zo);
   V.dl = __dsub_rn(__dsub_rn(dlay, __ldg(&E->foc)), __ldg(&E->steer));
   V.w = __ldg(&E->wvds);
+  const double bound = ((fabs(V.xo) + fabs(V.yo) + fabs(V.zo) + P.ab) * fabs(P.c1) + fabs(V.dl)) * fabs(P.inv_dt);
+  V.fast = !P.full && bound < RECT_WIN_TRUST;
 }
 
 // Sample index of a term at distance r, as the kernel computes it.
@@ -110,11 +120,10 @@ __device__ __forceinline__ double rect_q(double r, double dl, const RectParams &
 // to its nearest point and to its farthest corner. Unbounded where the
 // margin is not proven (or in the repeated launch).
 __device__ __forceinline__ bool elem_window(const RectParams &P, const ElemView &V, int64_t &lo, int64_t &hi) {
-  const double ax = fabs(V.xo), ay = fabs(V.yo), az = fabs(V.zo);
+  const double ax = fabs(V.xo), ay = fabs(V.yo);
   const double ex = fmax(ax - P.half_a, 0.0), ey = fmax(ay - P.half_b, 0.0);
   const double fx = ax + P.half_a, fy = ay + P.half_b;
-  const double bound = ((ax + ay + az + 2.0 * (P.half_a + P.half_b)) * 1000.0 / fabs(P.cp) + fabs(V.dl)) / fabs(P.dt);
-  if (P.full || !(bound < RECT_WIN_TRUST)) {
+  if (!V.fast) {
     lo = 0;
     hi = P.nt;
     return true;
@@ -153,7 +162,13 @@ __device__ __forceinline__ void term_step(const RectParams &P, const ElemView &V
     ai = __ddiv_rn(V.w, __dmul_rn(RECT_TWO_PI, r));
     ai = __ddiv_rn(ai, P.dt);
     ai = __dmul_rn(ai, 1000.0);
-    it = __double2ll_rn(rect_q(r, V.dl, P));  // rint, ties to even
+    // rint((t - dl)/dt), ties to even: the estimate where it is certain, else the exact chain
+    const double qa = __dmul_rn(__dsub_rn(__dmul_rn(r, P.c1), V.dl), P.inv_dt);
+    const double na = rint(qa);
+    if (V.fast && fabs(qa - na) < RECT_Q_SAFE)
+      it = (int64_t)na;
+    else
+      it = __double2ll_rn(rect_q(r, V.dl, P));
     in = it >= 0 && it < P.nt;
     oob += in ? 0u : 1u;
     if (!in && last) flags |= RECT_LAST_OOB;
@@ -561,6 +576,9 @@ int rect_device(RectBuffers &rb, const double *dRo, int64_t No, double a, double
   P.half_b = b / 2.0;
   P.dt = dt;
   P.cp = cp;
+  P.c1 = 1000.0 / cp;
+  P.inv_dt = 1.0 / dt;
+  P.ab = std::fabs(a) + std::fabs(b);
   P.nt = nt;
   P.delay = ddelay;
   P.delay_multi = delay_type == DREAM_DELAY_MULTIPLE;
