@@ -128,8 +128,9 @@ __device__ __forceinline__ bool elem_window(const RectParams &P, const ElemView 
     hi = P.nt;
     return true;
   }
-  const double qa = rect_q(sqrt(ex * ex + ey * ey + V.rz2), V.dl, P);
-  const double qb = rect_q(sqrt(fx * fx + fy * fy + V.rz2), V.dl, P);
+  // sample estimates (within 2^-13 of the exact chain's, see RECT_Q_SAFE)
+  const double qa = (sqrt(ex * ex + ey * ey + V.rz2) * P.c1 - V.dl) * P.inv_dt;
+  const double qb = (sqrt(fx * fx + fy * fy + V.rz2) * P.c1 - V.dl) * P.inv_dt;
   const int64_t sa = __double2ll_rn(qa), sb = __double2ll_rn(qb);
   lo = min(sa, sb) - 2;
   hi = max(sa, sb) + 3;
@@ -149,19 +150,26 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 // the sample index changes monotonically on either side of the point's
 // projection) the leaders read their run from the warp's 32 staged
 // amplitudes, four per trip; otherwise they walk their member masks.
+// SKIP: steps with no term in the SIR skip the amplitudes and the sums (arrays,
+// whose live elements still place most terms outside short windows); without
+// it the amplitude divisions overlap the index computation.
+template <bool SKIP>
 __device__ __forceinline__ void term_step(const RectParams &P, const ElemView &V, bool valid, int ix, int iy,
                                           int lane, int64_t w0, int64_t w1, double *h, double *stage,
                                           unsigned long long &oob, unsigned int &flags, bool last) {
   bool in = false;
   int64_t it = 0;
+  double r = 1.0;  // idle lanes: a finite amplitude that is never added
   double ai = 0.0;
   if (valid) {
     const double rx = __dsub_rn(V.xo, __ldg(P.xs + ix));
     const double ry = __dsub_rn(V.yo, __ldg(P.ys + iy));
-    const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), V.rz2));
-    ai = __ddiv_rn(V.w, __dmul_rn(RECT_TWO_PI, r));
-    ai = __ddiv_rn(ai, P.dt);
-    ai = __dmul_rn(ai, 1000.0);
+    r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), V.rz2));
+    if (!SKIP) {
+      ai = __ddiv_rn(V.w, __dmul_rn(RECT_TWO_PI, r));
+      ai = __ddiv_rn(ai, P.dt);
+      ai = __dmul_rn(ai, 1000.0);
+    }
     // rint((t - dl)/dt), ties to even: the estimate where it is certain, else the exact chain
     const double qa = __dmul_rn(__dsub_rn(__dmul_rn(r, P.c1), V.dl), P.inv_dt);
     const double na = rint(qa);
@@ -175,6 +183,12 @@ __device__ __forceinline__ void term_step(const RectParams &P, const ElemView &V
     const bool inside = it >= w0 && it < w1;  // true whenever the window bound holds
     if (in && !inside) flags |= RECT_MISS;
     in = in && inside;
+  }
+  if (SKIP) {
+    if (!__any_sync(0xffffffffu, in)) return;  // no term of this step lands in the SIR
+    ai = __ddiv_rn(V.w, __dmul_rn(RECT_TWO_PI, r));
+    ai = __ddiv_rn(ai, P.dt);
+    ai = __dmul_rn(ai, 1000.0);
   }
   // lanes adding into the same sample form a group; the others get unique keys
   const unsigned long long key = in ? (unsigned long long)it : ~0ull - (unsigned long long)lane;
@@ -276,7 +290,7 @@ __global__ void __launch_bounds__(RECT_WARPS * 32) rect_kernel(const RectParams 
       int iy = lane / P.nx;
       int ix = lane - iy * P.nx;
       for (int64_t e0 = 0; e0 < E; e0 += 32) {
-        term_step(P, V, e0 + lane < E, ix, iy, lane, w0, w1, h, stage, oob, flags, true);
+        term_step<false>(P, V, e0 + lane < E, ix, iy, lane, w0, w1, h, stage, oob, flags, true);
         ix += 32;
         while (ix >= P.nx) {  // once for rows of 32 or more elements
           ix -= P.nx;
@@ -309,7 +323,7 @@ __global__ void __launch_bounds__(RECT_WARPS * 32) rect_kernel(const RectParams 
       bool last = rest && c0 + __ffs(rest) - 1 == P.M - 1;  // this lane's element is the array's last
       if (rest) elem_view(P, c0 + __ffs(rest) - 1, n, V);
       for (int64_t g0 = 0; g0 < total; g0 += 32) {
-        term_step(P, V, g0 + lane < total, ix, iy, lane, w0, w1, h, stage, oob, flags, last);
+        term_step<true>(P, V, g0 + lane < total, ix, iy, lane, w0, w1, h, stage, oob, flags, last);
         // advance by 32 terms without a division (once per wrap for rows of 32 or more)
         ix += 32;
         bool next = false;
