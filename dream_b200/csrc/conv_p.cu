@@ -284,13 +284,16 @@ extern "C" {
 
 int dream_conv_p_run_device(const double *dA, int64_t A_M, int64_t A_N, const double *dB, int64_t B_M, int64_t B_N,
                             double *dY, int mode, void *stream) {
+  DREAM_API_TRY
   int r = conv_shapes(A_M, A_N, B_M, B_N, mode);
   if (r) return r;
   return conv_device(dA, A_M, A_N, dB, B_M, B_N, dY, mode, (cudaStream_t)stream);
+  DREAM_API_CATCH
 }
 
 int dream_conv_p_run(const double *A, int64_t A_M, int64_t A_N, const double *B, int64_t B_M, int64_t B_N, double *Y,
                      int mode, int device) {
+  DREAM_API_TRY
   int r = conv_shapes(A_M, A_N, B_M, B_N, mode);
   if (r) return r;
   const int64_t NY = A_M + B_M - 1;
@@ -327,6 +330,7 @@ int dream_conv_p_run(const double *A, int64_t A_M, int64_t A_N, const double *B,
   if (e == cudaSuccess) e = cudaStreamSynchronize(cb.st);
   if (e != cudaSuccess) return done(set_last_error(DREAM_ERR_CUDA, cudaGetErrorString(e)));
   return done(0);
+  DREAM_API_CATCH
 }
 
 }  // extern "C"

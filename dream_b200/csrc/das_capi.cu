@@ -17,6 +17,9 @@
 
 #include "../../include/dream_das.h"
 #include "das_fast.h"
+#include <exception>
+#include <new>
+
 #include "das_kernels.h"
 
 using namespace dream;
@@ -93,6 +96,25 @@ int status_from_oob(uint64_t oob, int err_level) {
 }  // namespace
 
 int dream::set_last_error(int code, const std::string &msg) { return fail(code, msg); }
+
+int dream::api_exception() noexcept {
+  int code = DREAM_ERR_ARGUMENT;
+  const char *msg = "unexpected C++ exception";
+  try {
+    throw;
+  } catch (const std::bad_alloc &) {
+    code = DREAM_ERR_ALLOC;
+    msg = "host memory allocation failed";
+  } catch (const std::exception &e) {
+    msg = e.what();
+  } catch (...) {
+  }
+  try {
+    g_last_error = msg;
+  } catch (...) {  // no memory even for the message: keep the old one
+  }
+  return code;
+}
 
 struct dream_das_plan {
   int das_type = 0;
@@ -432,6 +454,7 @@ const char *dream_das_last_error(void) { return g_last_error.c_str(); }
 
 int dream_das_plan_create(dream_das_plan **plan, int das_type, int64_t a_scan_len, int64_t No,
                           int64_t num_t_elements, int64_t num_r_elements, int precision, int device) {
+  DREAM_API_TRY
   if (plan == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan pointer is NULL");
   *plan = nullptr;
   int r = check_common(das_type, a_scan_len, No, num_t_elements, num_r_elements, precision);
@@ -464,16 +487,19 @@ int dream_das_plan_create(dream_das_plan **plan, int das_type, int64_t a_scan_le
   cudaDeviceGetAttribute(&p->sm_count, cudaDevAttrMultiProcessorCount, device);
   *plan = p;
   return 0;
+  DREAM_API_CATCH
 }
 
 int dream_das_setup_has_changed(const dream_das_plan *p, int das_type, int64_t a_scan_len, int64_t No,
                                 int64_t num_t_elements, int64_t num_r_elements, int precision, int device) {
+  DREAM_API_TRY
   if (p == nullptr) return 1;
   int64_t nr = (das_type == DREAM_DAS_SAFT) ? 0 : num_r_elements;
   return (p->uni || das_type != p->das_type || a_scan_len != p->K || No != p->No || num_t_elements != p->Nt ||
           nr != p->Nr || precision != p->precision || device != p->device)
              ? 1
              : 0;
+  DREAM_API_CATCH
 }
 
 void dream_das_plan_destroy(dream_das_plan *p) {
@@ -515,7 +541,10 @@ int64_t dream_das_plan_num_ascans(const dream_das_plan *p) { return p ? num_colu
 
 int64_t dream_das_plan_launch_count(const dream_das_plan *p) { return p ? p->launches.load() : -1; }
 
-int dream_das_checked_build(void) { return kChecked ? 1 : 0; }
+int dream_das_checked_build(void) {
+  DREAM_API_TRY return kChecked ? 1 : 0;
+  DREAM_API_CATCH
+}
 
 int64_t dream_das_plan_bound_violations(dream_das_plan *p) {
   if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
@@ -529,6 +558,7 @@ int64_t dream_das_plan_bound_violations(dream_das_plan *p) {
 }
 
 int dream_das_set_grid_hint(dream_das_plan *p, int64_t n_fast) {
+  DREAM_API_TRY
   if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
   if (n_fast < 0 || (n_fast > 0 && (p->No % n_fast) != 0))
     return fail(DREAM_ERR_ARGUMENT, "grid hint must divide the number of image points");
@@ -536,9 +566,11 @@ int dream_das_set_grid_hint(dream_das_plan *p, int64_t n_fast) {
   if (n_fast != p->n_fast) p->tile_f = p->tile_s = 0;  // tile shapes depend on the hint
   p->n_fast = n_fast;
   return 0;
+  DREAM_API_CATCH
 }
 
 int dream_das_set_tile(dream_das_plan *p, int tile_f, int tile_s) {
+  DREAM_API_TRY
   if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
   std::lock_guard<std::mutex> lk(p->mu);
   if (tile_f == 0 && tile_s == 0) {
@@ -553,33 +585,41 @@ int dream_das_set_tile(dream_das_plan *p, int tile_f, int tile_s) {
   p->tile_f = tile_f;
   p->tile_s = tile_s;
   return 0;
+  DREAM_API_CATCH
 }
 
 int dream_das_set_l2_block(dream_das_plan *p, int64_t bytes) {
+  DREAM_API_TRY
   if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
   std::lock_guard<std::mutex> lk(p->mu);
   p->l2_block = bytes;
   return 0;
+  DREAM_API_CATCH
 }
 
 int dream_das_set_chunk(dream_das_plan *p, int jc) {
+  DREAM_API_TRY
   if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
   if (jc != 0 && jc != 8 && jc != 16) return fail(DREAM_ERR_ARGUMENT, "chunk must be 0, 8 or 16");
   std::lock_guard<std::mutex> lk(p->mu);
   p->jc = jc;
   return 0;
+  DREAM_API_CATCH
 }
 
 int dream_das_get_tile(const dream_das_plan *p, int *tile_f, int *tile_s) {
+  DREAM_API_TRY
   if (p == nullptr || tile_f == nullptr || tile_s == nullptr) return fail(DREAM_ERR_ARGUMENT, "NULL argument");
   int wf = 0;
   const int n_out = (effective_method(p) == DREAM_DAS_RCA_ROWTX) ? (int)p->Nr : (int)p->Nt;
   fast_tile(p, n_out, *tile_f, *tile_s, wf);
   return 0;
+  DREAM_API_CATCH
 }
 
 int dream_das_bind_geometry(dream_das_plan *p, const void *dRo, const void *dGt, const void *dGr, double dt,
                             int delay_type, const void *ddelay, double cp, void *stream) {
+  DREAM_API_TRY
   if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
   if (p->precision != DREAM_PREC_F32_STORE || p->uni)
     return fail(DREAM_ERR_UNSUPPORTED, "the differentiable operator needs an F32_STORE plan");
@@ -622,6 +662,7 @@ int dream_das_bind_geometry(dream_das_plan *p, const void *dRo, const void *dGt,
   p->geo = F;
   p->bound = true;
   return 0;
+  DREAM_API_CATCH
 }
 
 static int op_check(dream_das_plan *p) {
@@ -633,6 +674,7 @@ static int op_check(dream_das_plan *p) {
 
 int dream_das_op_forward(dream_das_plan *p, const float *dY, const float *dW, float *dIm, unsigned long long *d_oob,
                          void *stream) {
+  DREAM_API_TRY
   int r = op_check(p);
   if (r) return r;
   std::lock_guard<std::mutex> lk(p->mu);
@@ -648,6 +690,7 @@ int dream_das_op_forward(dream_das_plan *p, const float *dY, const float *dW, fl
                        (cudaStream_t)stream));
   p->launches++;
   return 0;
+  DREAM_API_CATCH
 }
 
 static int op_colowner(dream_das_plan *p, const float *X, const float *G, const float *dY, const float *dW, float *Ya,
@@ -668,25 +711,30 @@ static int op_colowner(dream_das_plan *p, const float *X, const float *G, const 
 }
 
 int dream_das_op_adjoint(dream_das_plan *p, const float *dX, const float *dW, float *dYa, void *stream) {
+  DREAM_API_TRY
   int r = op_check(p);
   if (r) return r;
   if (dX == nullptr || dYa == nullptr) return fail(DREAM_ERR_ARGUMENT, "NULL device pointer");
   std::lock_guard<std::mutex> lk(p->mu);
   DeviceGuard g(p->device);
   return op_colowner(p, dX, nullptr, nullptr, dW, dYa, nullptr, true, false, (cudaStream_t)stream);
+  DREAM_API_CATCH
 }
 
 int dream_das_op_wgrad(dream_das_plan *p, const float *dG, const float *dY, float *dWgrad, void *stream) {
+  DREAM_API_TRY
   int r = op_check(p);
   if (r) return r;
   if (dG == nullptr || dY == nullptr || dWgrad == nullptr) return fail(DREAM_ERR_ARGUMENT, "NULL device pointer");
   std::lock_guard<std::mutex> lk(p->mu);
   DeviceGuard g(p->device);
   return op_colowner(p, nullptr, dG, dY, nullptr, nullptr, dWgrad, false, true, (cudaStream_t)stream);
+  DREAM_API_CATCH
 }
 
 int dream_das_op_backward(dream_das_plan *p, const float *dG, const float *dY, const float *dW, float *dYgrad,
                           float *dWgrad, void *stream) {
+  DREAM_API_TRY
   int r = op_check(p);
   if (r) return r;
   if (dG == nullptr || dYgrad == nullptr || dWgrad == nullptr || dY == nullptr)
@@ -694,6 +742,7 @@ int dream_das_op_backward(dream_das_plan *p, const float *dG, const float *dY, c
   std::lock_guard<std::mutex> lk(p->mu);
   DeviceGuard g(p->device);
   return op_colowner(p, dG, dG, dY, dW, dYgrad, dWgrad, true, true, (cudaStream_t)stream);
+  DREAM_API_CATCH
 }
 
 }  // extern "C"
@@ -714,6 +763,7 @@ struct dream_das_batch {
 extern "C" {
 
 int dream_das_batch_create(dream_das_batch **out, const dream_das_frame *fr, int n_frames, int precision, int device) {
+  DREAM_API_TRY
   if (out == nullptr || (fr == nullptr && n_frames > 0) || n_frames < 0) return fail(DREAM_ERR_ARGUMENT, "NULL argument");
   *out = nullptr;
   if (precision != DREAM_PREC_F32_STORE && precision != DREAM_PREC_BF16_STORE)
@@ -829,9 +879,11 @@ int dream_das_batch_create(dream_das_batch **out, const dream_das_frame *fr, int
   b->last_oob = (unsigned long long *)1;  // force the first upload
   *out = b;
   return 0;
+  DREAM_API_CATCH
 }
 
 int dream_das_batch_run(dream_das_batch *b, unsigned long long *d_oob, void *stream) {
+  DREAM_API_TRY
   if (b == nullptr) return fail(DREAM_ERR_ARGUMENT, "batch is NULL");
   std::lock_guard<std::mutex> lk(b->mu);
   DeviceGuard g(b->device);
@@ -847,11 +899,15 @@ int dream_das_batch_run(dream_das_batch *b, unsigned long long *d_oob, void *str
   CU(launch_batch((const FastParams *)b->bFrames.p, (const int4 *)b->bItems.p, (int)b->n_items, (int *)b->bCtr.p,
                   std::max<size_t>(b->smem, 1024), b->bf16, b->grid, st));
   return 0;
+  DREAM_API_CATCH
 }
 
 int64_t dream_das_batch_items(const dream_das_batch *b) { return b ? b->n_items : -1; }
 
-int dream_das_batch_grid(const dream_das_batch *b) { return b ? b->grid : -1; }
+int dream_das_batch_grid(const dream_das_batch *b) {
+  DREAM_API_TRY return b ? b->grid : -1;
+  DREAM_API_CATCH
+}
 
 void dream_das_batch_destroy(dream_das_batch *b) {
   if (b == nullptr) return;
@@ -867,6 +923,7 @@ void dream_das_batch_destroy(dream_das_batch *b) {
 int dream_das_weighted_run_device(dream_das_plan *p, const void *dY, const void *dRo, const void *dGt,
                                   const void *dGr, double dt, int delay_type, const void *ddelay, double cp,
                                   const float *dW, float *dIm, unsigned long long *d_oob, void *stream) {
+  DREAM_API_TRY
   if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
   if (!is_fast(p) || p->uni)
     return fail(DREAM_ERR_UNSUPPORTED, "weighted DAS needs an F32_STORE or BF16_STORE plan");
@@ -875,6 +932,7 @@ int dream_das_weighted_run_device(dream_das_plan *p, const void *dY, const void 
   std::lock_guard<std::mutex> lk(p->mu);
   DeviceGuard g(p->device);
   return launch_fast_plan(p, dY, dRo, dGt, dGr, dt, delay_type, ddelay, cp, dW, dIm, d_oob, (cudaStream_t)stream);
+  DREAM_API_CATCH
 }
 
 static int run_device_impl(dream_das_plan *p, const void *dY, const void *dRo, const void *dGt, const void *dGr,
@@ -893,6 +951,7 @@ static int run_device_impl(dream_das_plan *p, const void *dY, const void *dRo, c
 int dream_das_indices_device(dream_das_plan *p, const void *dRo, const void *dGt, const void *dGr, double dt,
                              int delay_type, const void *ddelay, double cp, int64_t *d_idx, int64_t *oob_count,
                              void *stream) {
+  DREAM_API_TRY
   if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
   if (p->uni) return fail(DREAM_ERR_ARGUMENT, "uniform-grid plan passed to dream_das_indices_device");
   if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
@@ -955,11 +1014,13 @@ int dream_das_indices_device(dream_das_plan *p, const void *dRo, const void *dGt
     *oob_count = (int64_t)h;
   }
   return 0;
+  DREAM_API_CATCH
 }
 
 int dream_das_run_device(dream_das_plan *p, const void *dY, const void *dRo, const void *dGt, const void *dGr,
                          double dt, int delay_type, const void *ddelay, double cp, void *dIm, int err_level,
                          int64_t *oob_count, void *stream) {
+  DREAM_API_TRY
   if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
   if (p->uni) return fail(DREAM_ERR_ARGUMENT, "uniform-grid plan passed to dream_das_run_device");
   if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
@@ -975,11 +1036,13 @@ int dream_das_run_device(dream_das_plan *p, const void *dY, const void *dRo, con
   uint64_t oob = *p->h_oob;
   if (oob_count) *oob_count = (int64_t)oob;
   return status_from_oob(oob, err_level);
+  DREAM_API_CATCH
 }
 
 int dream_das_run_device_async(dream_das_plan *p, const void *dY, const void *dRo, const void *dGt,
                                const void *dGr, double dt, int delay_type, const void *ddelay, double cp,
                                void *dIm, unsigned long long *d_oob, void *stream) {
+  DREAM_API_TRY
   if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
   if (p->uni) return fail(DREAM_ERR_ARGUMENT, "uniform-grid plan passed to dream_das_run_device_async");
   if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
@@ -987,6 +1050,7 @@ int dream_das_run_device_async(dream_das_plan *p, const void *dY, const void *dR
   DeviceGuard g(p->device);
   cudaStream_t st = (cudaStream_t)stream;  // NULL: the default stream
   return run_device_impl(p, dY, dRo, dGt, dGr, dt, delay_type, ddelay, cp, dIm, d_oob, st);
+  DREAM_API_CATCH
 }
 
 // Inner-element boundaries of the pipelined upload: UPLOAD_CHUNKS ranges on
@@ -1008,6 +1072,7 @@ static std::vector<int> upload_chunks(int n_in) {
 
 int dream_das_run(dream_das_plan *p, const void *Y, const void *Ro, const void *Gt, const void *Gr, double dt,
                   int delay_type, const void *delay, double cp, void *Im, int err_level, int64_t *oob_count) {
+  DREAM_API_TRY
   if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
   if (p->uni) return fail(DREAM_ERR_ARGUMENT, "uniform-grid plan passed to dream_das_run");
   if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
@@ -1099,6 +1164,7 @@ int dream_das_run(dream_das_plan *p, const void *Y, const void *Ro, const void *
   uint64_t oob = *p->h_oob;
   if (oob_count) *oob_count = (int64_t)oob;
   return status_from_oob(oob, err_level);
+  DREAM_API_CATCH
 }
 
 // ---------------------------------------------------------------------------
@@ -1107,6 +1173,7 @@ int dream_das_run(dream_das_plan *p, const void *Y, const void *Ro, const void *
 
 int dream_das_uni_plan_create(dream_das_plan **plan, int das_type, int64_t a_scan_len, const double *tri,
                               int precision, int device) {
+  DREAM_API_TRY
   if (plan == nullptr || tri == nullptr) return fail(DREAM_ERR_ARGUMENT, "NULL argument");
   *plan = nullptr;
   if (precision != DREAM_PREC_F64 && precision != DREAM_PREC_F32)
@@ -1130,6 +1197,7 @@ int dream_das_uni_plan_create(dream_das_plan **plan, int das_type, int64_t a_sca
   p->Ny = Ny;
   p->Nz = Nz;
   return 0;
+  DREAM_API_CATCH
 }
 
 static int uni_launch(dream_das_plan *p, const void *dY, const double *tri, double dt, double delay, double cp,
@@ -1166,6 +1234,7 @@ static int uni_launch(dream_das_plan *p, const void *dY, const double *tri, doub
 
 int dream_das_uni_run_device(dream_das_plan *p, const void *dY, const double *tri, double dt, double delay,
                              double cp, void *dIm, int err_level, int64_t *oob_count, void *stream) {
+  DREAM_API_TRY
   if (p == nullptr || !p->uni) return fail(DREAM_ERR_ARGUMENT, "not a uniform-grid plan");
   if (tri == nullptr) return fail(DREAM_ERR_ARGUMENT, "tri is NULL");
   if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
@@ -1181,10 +1250,12 @@ int dream_das_uni_run_device(dream_das_plan *p, const void *dY, const double *tr
   uint64_t oob = *p->h_oob;
   if (oob_count) *oob_count = (int64_t)oob;
   return status_from_oob(oob, err_level);
+  DREAM_API_CATCH
 }
 
 int dream_das_uni_run(dream_das_plan *p, const void *Y, const double *tri, double dt, double delay, double cp,
                       void *Im, int err_level, int64_t *oob_count) {
+  DREAM_API_TRY
   if (p == nullptr || !p->uni) return fail(DREAM_ERR_ARGUMENT, "not a uniform-grid plan");
   if (tri == nullptr) return fail(DREAM_ERR_ARGUMENT, "tri is NULL");
   if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
@@ -1207,6 +1278,7 @@ int dream_das_uni_run(dream_das_plan *p, const void *Y, const double *tri, doubl
   uint64_t oob = *p->h_oob;
   if (oob_count) *oob_count = (int64_t)oob;
   return status_from_oob(oob, err_level);
+  DREAM_API_CATCH
 }
 
 }  // extern "C"

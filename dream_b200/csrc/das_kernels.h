@@ -49,6 +49,18 @@ cudaError_t launch_plain_f64(const PlainLaunch &L, cudaStream_t st);
 // Records msg as this host thread's last error (dream_das_last_error) and
 // returns code.
 int set_last_error(int code, const std::string &msg);
+
+// The status of the C++ exception being handled (call only inside a catch
+// block): DREAM_ERR_ALLOC for std::bad_alloc, DREAM_ERR_ARGUMENT otherwise,
+// with its message recorded. Every int-returning C ABI entry wraps its body in
+// DREAM_API_TRY ... DREAM_API_CATCH, so no exception crosses the C boundary.
+int api_exception() noexcept;
+#define DREAM_API_TRY try {
+#define DREAM_API_CATCH \
+  }                     \
+  catch (...) {         \
+    return ::dream::api_exception(); \
+  }
 cudaError_t launch_plain_f32(const PlainLaunch &L, cudaStream_t st);
 
 }  // namespace dream

@@ -59,6 +59,7 @@ cudaError_t noalloc_scratch_ptr(int device, void **ptr) {
 
 extern "C" int dream_das_batch_run_noalloc(const dream_das_frame *fr, int n_frames, int precision, int device,
                                            unsigned long long *d_oob, void *stream) {
+  DREAM_API_TRY
   using namespace dream;
   if ((fr == nullptr && n_frames > 0) || n_frames < 0) return set_last_error(DREAM_ERR_ARGUMENT, "NULL argument");
   if (precision != DREAM_PREC_F32_STORE && precision != DREAM_PREC_BF16_STORE)
@@ -189,4 +190,5 @@ extern "C" int dream_das_batch_run_noalloc(const dream_das_frame *fr, int n_fram
                    (int)n_items, reinterpret_cast<int *>(base), smem, bf16, grid, st);
   if (e != cudaSuccess) return set_last_error(DREAM_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
   return 0;
+  DREAM_API_CATCH
 }

@@ -727,15 +727,19 @@ ArrDesc arr_desc(int64_t num_elements, const double *G, int foc_met, const doubl
 int dream_rect_run_device(const double *dRo, int64_t No, double a, double b, double dx, double dy, double dt,
                           int64_t nt, int delay_type, const double *ddelay, double v, double cp, double *dH,
                           int err_level, int64_t *oob_count, int device, void *stream) {
+  DREAM_API_TRY
   return rect_entry_device(dRo, No, a, b, dx, dy, dt, nt, delay_type, ddelay, v, cp, ArrDesc(), dH, err_level,
                            oob_count, device, stream);
+  DREAM_API_CATCH
 }
 
 int dream_rect_run(const double *Ro, int64_t No, double a, double b, double dx, double dy, double dt, int64_t nt,
                    int delay_type, const double *delay, double v, double cp, double *H, int err_level,
                    int64_t *oob_count, int device) {
+  DREAM_API_TRY
   return rect_entry_host(Ro, No, a, b, dx, dy, dt, nt, delay_type, delay, v, cp, ArrDesc(), H, err_level, oob_count,
                          device);
+  DREAM_API_CATCH
 }
 
 int dream_arr_rect_run_device(const double *dRo, int64_t No, double a, double b, double dx, double dy, double dt,
@@ -744,10 +748,12 @@ int dream_arr_rect_run_device(const double *dRo, int64_t No, double a, double b,
                               int steer_met, double theta, double phi, int apod_met, const double *apod,
                               double apod_par, double *dH, int err_level, int64_t *oob_count, int device,
                               void *stream) {
+  DREAM_API_TRY
   if (num_elements > 0 && G == nullptr) return set_last_error(DREAM_ERR_ARGUMENT, "dream_arr_rect: NULL element grid");
   return rect_entry_device(dRo, No, a, b, dx, dy, dt, nt, delay_type, ddelay, v, cp,
                            arr_desc(num_elements, G, foc_met, focal, steer_met, theta, phi, apod_met, apod, apod_par),
                            dH, err_level, oob_count, device, stream);
+  DREAM_API_CATCH
 }
 
 int dream_arr_rect_run(const double *Ro, int64_t No, double a, double b, double dx, double dy, double dt,
@@ -755,10 +761,12 @@ int dream_arr_rect_run(const double *Ro, int64_t No, double a, double b, double 
                        const double *G, int foc_met, const double *focal, int steer_met, double theta, double phi,
                        int apod_met, const double *apod, double apod_par, double *H, int err_level,
                        int64_t *oob_count, int device) {
+  DREAM_API_TRY
   if (num_elements > 0 && G == nullptr) return set_last_error(DREAM_ERR_ARGUMENT, "dream_arr_rect: NULL element grid");
   return rect_entry_host(Ro, No, a, b, dx, dy, dt, nt, delay_type, delay, v, cp,
                          arr_desc(num_elements, G, foc_met, focal, steer_met, theta, phi, apod_met, apod, apod_par),
                          H, err_level, oob_count, device);
+  DREAM_API_CATCH
 }
 
 }  // extern "C"

@@ -136,3 +136,19 @@ def test_empty_shapes():
     assert H.shape == (c["nt"], 0)
     H = _call(dict(c, nt=0), "ignore")
     assert H.shape == (0, c["Ro"].shape[0])
+
+
+def test_host_exception_becomes_a_status():
+    # 2^60 elements: the element table's std::vector throws length_error before
+    # any allocation (and before the grid is read); the C ABI returns an error
+    from dream_b200 import _lib
+    L = _lib.load()
+    G = np.zeros((1, 3), order="F")
+    Ro = np.asfortranarray([[0.0, 0.0, 5.0]])
+    d = np.zeros(1)
+    H = np.zeros((10, 1), order="F")
+    p = lambda x: x.ctypes.data_as(ctypes.c_void_p)
+    st = L.dream_arr_rect_run(p(Ro), 1, 1.0, 1.0, 0.1, 0.1, 0.1, 10, 0, p(d), 1.0, 1500.0, 1 << 60, p(G), 0, p(d),
+                              0, 0.0, 0.0, 0, None, 0.0, p(H), 1, None, 0)
+    assert st == _lib.ERR_ARGUMENT
+    assert L.dream_das_last_error()
