@@ -498,25 +498,38 @@ def sir_bench(dev, cpu_sample: bool = True):
     del Rd
     torch.cuda.empty_cache()
     if cpu_sample:
+        from concurrent.futures import ThreadPoolExecutor
+
         from oracle import oracle
+        cores = len(os.sched_getaffinity(0))
+
+        def threaded(fn, pts):
+            # one block of points per host thread (the calls release the GIL)
+            blocks = [np.asfortranarray(b) for b in np.array_split(pts, cores) if len(b)]
+            t0 = time.perf_counter()
+            with ThreadPoolExecutor(cores) as ex:
+                res = list(ex.map(fn, blocks))
+            return time.perf_counter() - t0, res
+
         Ro, g, sp, mp, n_el, _ = cfgs["bench_dreamrect"]
-        sample = Ro[:: Ro.shape[0] // 16][:16]
-        t0 = time.perf_counter()
-        R = oracle.reference_rect(sample, g[0], g[1], sp[0], sp[1], sp[2], sp[3], 0.0, mp[0], mp[1])
-        dt_cpu = time.perf_counter() - t0
-        if R is not None:
-            out["cpu_baseline"] = {"gterms_s": 16 * n_el / dt_cpu / 1e9, "cores": 1, "kind": "reference",
-                                   "sample": "16 points of bench_dreamrect through the reference's "
-                                             "opencl/dreamrect.cl compiled as C (oracle/_ref, one thread)"}
-        sample = arr["Ro"][:: arr["Ro"].shape[0] // 512][:512]
-        t0 = time.perf_counter()
-        oracle.arr_rect(sample, arr["geom"][0], arr["geom"][1], arr["G"], arr["s_par"][0], arr["s_par"][1],
-                        arr["s_par"][2], arr["s_par"][3], arr["delay"], 1.0, 1500.0, "xy", 50.0, "x", -25.0, 0.0)
-        dt_cpu = time.perf_counter() - t0
+        n_s = 16 * cores
+        sample = Ro[:: Ro.shape[0] // n_s][:n_s]
+        dt_cpu, res = threaded(lambda b: oracle.reference_rect(b, g[0], g[1], sp[0], sp[1], sp[2], sp[3], 0.0, mp[0],
+                                                               mp[1]), sample)
+        if res and res[0] is not None:
+            out["cpu_baseline"] = {"gterms_s": n_s * n_el / dt_cpu / 1e9, "cores": cores, "kind": "reference",
+                                   "sample": f"{n_s} points of bench_dreamrect through the reference's "
+                                             f"opencl/dreamrect.cl compiled as C (oracle/_ref), {cores} host threads "
+                                             "over blocks of points, as the reference's CPU dreamrect threads"}
+        n_s = 128 * cores
+        sample = arr["Ro"][:: arr["Ro"].shape[0] // n_s][:n_s]
+        dt_cpu, _ = threaded(lambda b: oracle.arr_rect(b, arr["geom"][0], arr["geom"][1], arr["G"], arr["s_par"][0],
+                                                       arr["s_par"][1], arr["s_par"][2], arr["s_par"][3],
+                                                       arr["delay"], 1.0, 1500.0, "xy", 50.0, "x", -25.0, 0.0), sample)
         out["rect_arr_example"]["cpu_baseline"] = {
-            "gterms_s": 512 * arr["M"] * arr["n_el"] / dt_cpu / 1e9, "cores": 1, "kind": "port",
-            "sample": "512 points of rect_arr_example through the oracle's dream_arr_rect (one thread; the "
-                      "reference's CPU dream_arr_rect needs FFTW and is not built here)"}
+            "gterms_s": n_s * arr["M"] * arr["n_el"] / dt_cpu / 1e9, "cores": cores, "kind": "port",
+            "sample": f"{n_s} points of rect_arr_example through the oracle's dream_arr_rect, {cores} host threads "
+                      "over blocks of points (the reference's CPU dream_arr_rect needs FFTW and is not built here)"}
     out["note"] = "wall time around the call (includes the status read-back); unit = one surface-element term"
     return out
 

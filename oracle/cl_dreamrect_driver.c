@@ -5,7 +5,7 @@
  * the build is the unmodified reference kernel, used to pin
  * dream_oracle_rect (rect_oracle.c) and to generate tests/golden/rect_golden.npz.
  */
-int dream_ref_gid;
+__thread int dream_ref_gid;
 
 void dreamrect(const double *Ro, int No, double a, double b, double dx, double dy, double dt, int nt,
                double delay, double v, double cp, double *H);
