@@ -70,3 +70,17 @@ def test_error_levels(capsys):
         _call(c, "stop")
     H = _call(RECT_CASES["tfm_test_line"], "stop")  # nothing out of bounds: no error
     assert H.shape == (2000, 31)
+
+
+@pytest.mark.parametrize("seed", range(24))
+def test_random_elements_match_oracle(seed):
+    # seeded random element, discretisation, sampling and points (one delay or one per point)
+    rng = np.random.default_rng(100 + seed)
+    a, b = rng.uniform(0.05, 12.0, 2)
+    c = dict(Ro=np.asfortranarray(np.stack([rng.uniform(-15, 15, 20), rng.uniform(-15, 15, 20),
+                                            rng.uniform(0.1, 40, 20)], 1)),
+             a=a, b=b, dx=a / rng.integers(1, 120), dy=b / rng.integers(1, 120), dt=float(rng.choice([0.01, 0.05, 0.25])),
+             nt=int(rng.integers(1, 3000)), v=float(rng.uniform(0.5, 2)), cp=float(rng.uniform(1000, 6000)))
+    d = np.full((1, 1), rng.uniform(-3, 10)) if rng.random() < 0.6 else rng.uniform(-3, 10, (20, 1))
+    ref, _, _ = oracle.rect(c["Ro"], c["a"], c["b"], c["dx"], c["dy"], c["dt"], c["nt"], d, c["v"], c["cp"], "ignore")
+    assert np.array_equal(_call(c, delay=d), ref)
