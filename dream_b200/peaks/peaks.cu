@@ -1,5 +1,5 @@
 // peaks.cu -- microbenchmarks for the roofline denominators the DAS kernels are
-// judged against on this GPU (built into libdream_peaks.so, run by
+// measured against on this GPU (built into libdream_peaks.so, run by
 // `python bench.py --peaks`; not part of the beamformer library):
 //
 //   l2_sector_gather  one 4-byte load per thread at a random 32-byte sector of
