@@ -407,11 +407,20 @@ def conv_bench(dev, cpu_sample: bool = True):
     with torch.cuda.graph(g):
         synth()
     ms = timed(g.replay)
+    del g
+    # every transmit in two launches (dream_b200.conv.fmc_synthesis), the same A-scans bit for bit
+    from dream_b200.conv import fmc_synthesis
+    ref_cols = Yfmc[:, 50 * L:51 * L].clone()
+    ms_batched = timed(lambda: fmc_synthesis(H, h_e))
+    if not torch.equal(fmc_synthesis(H, h_e)[:, 50 * L:51 * L], ref_cols):
+        raise RuntimeError("fmc_synthesis differs from the per-transmit fftconv_p calls")
     macs = L * (nt * nt * L + (2 * nt - 1) * nt_he * L)
     out = {"config": "FMC synthesis, 101 elements, SIR 2000 samples, pulse 150 samples, FP64 (reference TFM test)",
            "macs": macs, "ms": ms, "gmac_s": macs / ms / 1e6, "ms_eager": ms_eager,
+           "ms_batched": ms_batched, "gmac_s_batched": macs / ms_batched / 1e6,
            "note": "bit-identical to the reference's direct conv(); FFTW's fftconv_p differs by rounding; "
-                   "ms: the 202 launches replayed from a CUDA graph, ms_eager: issued from Python"}
+                   "ms: the reference's 202 fftconv_p calls replayed from a CUDA graph, ms_eager: issued from "
+                   "Python, ms_batched: all transmits in two launches (fmc_synthesis)"}
     if cpu_sample:
         from concurrent.futures import ThreadPoolExecutor
 

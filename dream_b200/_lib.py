@@ -61,6 +61,7 @@ SIGNATURES = {
     "dream_das_indices_device": (_i, [_vp, _vp, _vp, _vp, _d, _i, _vp, _d, _vp, _vp, _vp]),
     "dream_conv_p_run_device": (_i, [_vp, _i64, _i64, _vp, _i64, _i64, _vp, _i, _vp]),
     "dream_conv_p_run": (_i, [_vp, _i64, _i64, _vp, _i64, _i64, _vp, _i, _i]),
+    "dream_conv_p_fmc_device": (_i, [_vp, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _vp, _vp]),
     "dream_rect_run_device": (_i, [_vp, _i64, _d, _d, _d, _d, _d, _i64, _i, _vp, _d, _d, _vp, _i, _vp, _i, _vp]),
     "dream_rect_run": (_i, [_vp, _i64, _d, _d, _d, _d, _d, _i64, _i, _vp, _d, _d, _vp, _i, _vp, _i]),
     "dream_arr_rect_run_device": (_i, [_vp, _i64, _d, _d, _d, _d, _d, _i64, _i, _vp, _d, _d, _i64, _vp, _i, _vp,

@@ -110,3 +110,34 @@ def conv_p(A, B, Y=None, mode="=", device="cuda"):
     elif not (isinstance(Y, np.ndarray) and Y.dtype == np.float64 and Y.flags["F_CONTIGUOUS"]):
         raise RuntimeError("conv_p: Y must be an F-order float64 array")
     return _run(A, B, Y, _MODES[mode], device)
+
+
+def fmc_synthesis(Ht, pulse, Hr=None, device="cuda"):
+    """Full-matrix-capture A-scans from element SIRs in two launches: column
+    ``t*L_r + r`` is ``(Hr[:, r] (*) Ht[:, t]) (*) pulse``, which the
+    reference's tests build with two fftconv_p calls per transmit
+    (python/tests/test_das_tfm.py:110-115, with Hr = Ht; test_das_rca.py:117-124).
+    Ht: M x L_t transmit SIRs, Hr: M x L_r receive SIRs (default Ht), pulse:
+    P_M samples. Returns (2M-1 + P_M-1) x L_t*L_r FP64 (column-major), equal
+    to the per-transmit calls bit for bit: a CUDA tensor when Ht is one, else
+    a NumPy array."""
+    import torch
+    on_device = _is_torch(Ht) and Ht.device.type == "cuda"
+    dev = Ht.device if on_device else torch.device("cuda", parse_device(device))
+    as_dev = lambda a: _device_fortran(a.to(dev) if _is_torch(a) else torch.as_tensor(np.asarray(a), device=dev))
+    Htd = as_dev(Ht)
+    Hrd = Htd if Hr is None else as_dev(Hr)
+    Pd = as_dev(pulse).reshape(-1).contiguous()
+    M, L_t = _dims(Htd)
+    M_r, L_r = _dims(Hrd)
+    if M_r != M:
+        raise RuntimeError("fmc_synthesis: the transmit and receive SIRs must have the same length")
+    P_M = Pd.numel()
+    N = L_t * L_r
+    DP = torch.empty((N, 2 * M - 1), dtype=torch.float64, device=dev).t()
+    Y = torch.empty((N, 2 * M - 1 + P_M - 1), dtype=torch.float64, device=dev).t()
+    p = lambda t: ctypes.c_void_p(t.data_ptr()) if t.numel() else None
+    st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    _lib.check(_lib.load().dream_conv_p_fmc_device(p(Htd), M, L_t, p(Hrd), L_r, p(Pd), P_M, p(DP), p(Y), st))
+    del DP  # stream-ordered release: the caching allocator reuses it only after the launches
+    return Y if on_device else Y.cpu().numpy()

@@ -94,10 +94,14 @@ __device__ __forceinline__ int64_t centre_out_tile(int64_t y, int64_t n) {
   return m - (y - hi);
 }
 
+// Column n of the output convolves A column n % na with B column n / nb
+// (na = N, nb = 1 for fftconv_p / conv_p; the full-matrix-capture synthesis
+// pairs every receive column with every transmit column).
 template <int MODE>
 __global__ void __launch_bounds__(CONV_WARPS * 32) conv_p_kernel(const double *__restrict__ A, int64_t M, int64_t N,
                                                                   const double *__restrict__ B, int64_t L,
-                                                                  int64_t ldb, double *__restrict__ Y, int64_t NY) {
+                                                                  int64_t ldb, double *__restrict__ Y, int64_t NY,
+                                                                  int64_t na, int64_t nb) {
   extern __shared__ __align__(16) double conv_sm[];
   double *ys = conv_sm;      // [L]
   double *xs = conv_sm + L;  // xs[conv_sw(q)] = A[k_cta - (L - 1) + q] (0 outside the column)
@@ -107,8 +111,8 @@ __global__ void __launch_bounds__(CONV_WARPS * 32) conv_p_kernel(const double *_
   const int64_t W = conv_window(L);
   const double neutral = MODE == 2 ? 0.0 : -0.0;
   for (int64_t n = blockIdx.x; n < N; n += gridDim.x) {
-    const double *x = A + n * M;
-    const double *y = B + n * ldb;
+    const double *x = A + (n % na) * M;
+    const double *y = B + (n / nb) * ldb;
     double *z = Y + n * NY;
     __syncthreads();  // the previous column's window is no longer read
     for (int64_t q = tid; q < L; q += blockDim.x) ys[q] = y[q];
@@ -183,12 +187,13 @@ __global__ void __launch_bounds__(CONV_WARPS * 32) conv_p_kernel(const double *_
 template <int MODE>
 __global__ void __launch_bounds__(256) conv_p_global_kernel(const double *__restrict__ A, int64_t M, int64_t N,
                                                              const double *__restrict__ B, int64_t L, int64_t ldb,
-                                                             double *__restrict__ Y, int64_t NY) {
+                                                             double *__restrict__ Y, int64_t NY, int64_t na,
+                                                             int64_t nb) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   for (int64_t n = blockIdx.y; n < N; n += gridDim.y) {
     if (k >= NY) continue;
-    const double *x = A + n * M;
-    const double *y = B + n * ldb;
+    const double *x = A + (n % na) * M;
+    const double *y = B + (n / nb) * ldb;
     double acc = MODE == 0 ? 0.0 : Y[n * NY + k];
     const int64_t i_lo = std::max<int64_t>(0, k - (L - 1)), i_hi = std::min<int64_t>(M - 1, k);
     for (int64_t i = i_lo; i <= i_hi; i++) acc = conv_acc<MODE>(acc, __dmul_rn(__ldg(x + i), __ldg(y + (k - i))));
@@ -198,7 +203,7 @@ __global__ void __launch_bounds__(256) conv_p_global_kernel(const double *__rest
 
 template <int MODE>
 cudaError_t launch_mode(const double *A, int64_t M, int64_t N, const double *B, int64_t L, int64_t ldb, double *Y,
-                        int64_t NY, cudaStream_t st) {
+                        int64_t NY, cudaStream_t st, int64_t na, int64_t nb) {
   const unsigned gy = (unsigned)std::min<int64_t>(N, 65535);
   if (L <= CONV_LMAX && (NY + CONV_T - 1) / CONV_T <= 65535) {
     const size_t smem = conv_smem_bytes(L);
@@ -207,10 +212,10 @@ cudaError_t launch_mode(const double *A, int64_t M, int64_t N, const double *B, 
     // x: columns (fastest, so every column's middle tile launches before any
     // column's edge tiles), y: tiles in centre-out order
     dim3 grid((unsigned)std::min<int64_t>(N, 1 << 30), (unsigned)((NY + CONV_T - 1) / CONV_T));
-    conv_p_kernel<MODE><<<grid, CONV_WARPS * 32, smem, st>>>(A, M, N, B, L, ldb, Y, NY);
+    conv_p_kernel<MODE><<<grid, CONV_WARPS * 32, smem, st>>>(A, M, N, B, L, ldb, Y, NY, na, nb);
   } else {
     dim3 grid((unsigned)((NY + 255) / 256), gy);
-    conv_p_global_kernel<MODE><<<grid, 256, 0, st>>>(A, M, N, B, L, ldb, Y, NY);
+    conv_p_global_kernel<MODE><<<grid, 256, 0, st>>>(A, M, N, B, L, ldb, Y, NY, na, nb);
   }
   return cudaGetLastError();
 }
@@ -246,9 +251,9 @@ int conv_device(const double *dA, int64_t A_M, int64_t A_N, const double *dB, in
   }
   if (dA == nullptr || dB == nullptr) return set_last_error(DREAM_ERR_ARGUMENT, "NULL input pointer");
   const int64_t ldb = B_N > 1 ? B_M : 0;
-  cudaError_t e = mode == DREAM_CONV_EQU   ? launch_mode<0>(dA, A_M, A_N, dB, B_M, ldb, dY, NY, st)
-                  : mode == DREAM_CONV_SUM ? launch_mode<1>(dA, A_M, A_N, dB, B_M, ldb, dY, NY, st)
-                                           : launch_mode<2>(dA, A_M, A_N, dB, B_M, ldb, dY, NY, st);
+  cudaError_t e = mode == DREAM_CONV_EQU   ? launch_mode<0>(dA, A_M, A_N, dB, B_M, ldb, dY, NY, st, A_N, 1)
+                  : mode == DREAM_CONV_SUM ? launch_mode<1>(dA, A_M, A_N, dB, B_M, ldb, dY, NY, st, A_N, 1)
+                                           : launch_mode<2>(dA, A_M, A_N, dB, B_M, ldb, dY, NY, st, A_N, 1);
   if (e != cudaSuccess) return set_last_error(DREAM_ERR_CUDA, std::string("conv_p launch: ") + cudaGetErrorString(e));
   return 0;
 }
@@ -330,6 +335,25 @@ int dream_conv_p_run(const double *A, int64_t A_M, int64_t A_N, const double *B,
   if (e == cudaSuccess) e = cudaStreamSynchronize(cb.st);
   if (e != cudaSuccess) return done(set_last_error(DREAM_ERR_CUDA, cudaGetErrorString(e)));
   return done(0);
+  DREAM_API_CATCH
+}
+
+int dream_conv_p_fmc_device(const double *dHt, int64_t M, int64_t L_t, const double *dHr, int64_t L_r,
+                            const double *dP, int64_t P_M, double *dDP, double *dY, void *stream) {
+  DREAM_API_TRY
+  if (M <= 0 || L_t < 0 || L_r < 0 || P_M <= 0)
+    return set_last_error(DREAM_ERR_ARGUMENT, "fmc synthesis: M and the pulse length must be positive");
+  const int64_t N = L_t * L_r;
+  if (N == 0) return 0;
+  if (dHt == nullptr || dHr == nullptr || dP == nullptr || dDP == nullptr || dY == nullptr)
+    return set_last_error(DREAM_ERR_ARGUMENT, "NULL pointer");
+  const cudaStream_t st = (cudaStream_t)stream;
+  const int64_t NY1 = 2 * M - 1, NY2 = NY1 + P_M - 1;
+  // double path: column t*L_r + r = Hr[:, r] (*) Ht[:, t]; then every column (*) the pulse
+  cudaError_t e = launch_mode<0>(dHr, M, N, dHt, M, M, dDP, NY1, st, L_r, L_r);
+  if (e == cudaSuccess) e = launch_mode<0>(dDP, NY1, N, dP, P_M, 0, dY, NY2, st, N, 1);
+  if (e != cudaSuccess) return set_last_error(DREAM_ERR_CUDA, std::string("fmc synthesis launch: ") + cudaGetErrorString(e));
+  return 0;
   DREAM_API_CATCH
 }
 

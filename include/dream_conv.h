@@ -43,6 +43,18 @@ int dream_conv_p_run_device(const double *dA, int64_t A_M, int64_t A_N, const do
 int dream_conv_p_run(const double *A, int64_t A_M, int64_t A_N, const double *B, int64_t B_M, int64_t B_N,
                      double *Y, int mode, int device);
 
+/* Full-matrix-capture A-scan synthesis in two launches (no reference entry:
+ * it batches the reference's per-transmit loop of fftconv_p calls,
+ * python/tests/test_das_tfm.py:110-115 and test_das_rca.py:117-124):
+ * column t*L_r + r of dY ((2M-1 + P_M-1) x L_t*L_r) is
+ * (dHr[:, r] (*) dHt[:, t]) (*) dP, with dHt M x L_t (transmit SIRs), dHr
+ * M x L_r (receive SIRs; dHt again for TFM), dP the P_M-sample pulse and dDP
+ * (2M-1) x L_t*L_r scratch for the double-path responses. Bit-identical to
+ * the two fftconv_p calls per transmit. Device buffers; asynchronous on
+ * `stream`. */
+int dream_conv_p_fmc_device(const double *dHt, int64_t M, int64_t L_t, const double *dHr, int64_t L_r,
+                            const double *dP, int64_t P_M, double *dDP, double *dY, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -111,3 +111,24 @@ def test_reference_tfm_synthesis_columns():
     Y = fftconv_p(Hdp, h_e)
     assert Y.shape == (4148, 101)
     assert np.array_equal(Y, oracle.conv_p(Hdp, h_e))
+
+
+@pytest.mark.parametrize("receive", ["same", "other"])
+def test_fmc_synthesis_equals_per_transmit_calls(receive):
+    # the reference tests' loop: two fftconv_p calls per transmit (TFM: Hr = Ht; RCA: separate receive SIRs)
+    from dream_b200.conv import fftconv_p, fmc_synthesis
+    rng = np.random.default_rng(8)
+    Ht = np.asfortranarray(rng.normal(size=(300, 7)))
+    Hr = Ht if receive == "same" else np.asfortranarray(rng.normal(size=(300, 5)))
+    pulse = rng.normal(size=40)
+    Y = fmc_synthesis(torch.from_numpy(np.ascontiguousarray(Ht.T)).cuda().t(), pulse,
+                      None if receive == "same" else torch.from_numpy(np.ascontiguousarray(Hr.T)).cuda().t())
+    L_r = Hr.shape[1]
+    assert tuple(Y.shape) == (2 * 300 - 1 + 40 - 1, 7 * L_r)
+    Yh = Y.cpu().numpy()
+    for t in range(7):
+        loop = fftconv_p(fftconv_p(Hr, Ht[:, t]), pulse)
+        assert np.array_equal(Yh[:, t * L_r:(t + 1) * L_r], loop)
+    assert np.array_equal(Yh[:, 3 * L_r:4 * L_r], oracle.conv_p(oracle.conv_p(Hr, Ht[:, 3]), pulse))
+    # host arrays in, host array out
+    assert np.array_equal(fmc_synthesis(Ht, pulse, None if receive == "same" else Hr), Yh)
