@@ -587,7 +587,7 @@ def batch_bench(dev, steps: int = 10, n_frames: int = 48):
 
 CASES = ("fast_f32", "fast_bf16", "plain_f64", "plain_f32", "saft_fast", "saft_plain_f64", "uni_f32",
          "batch", "op_gather", "op_adjoint", "op_wgrad", "op_backward", "rca_bf16", "rca_f32", "conv_dp", "conv_pulse",
-         "sir_field", "sir_arr")
+         "sir_field", "sir_arr", "conv_fmc")
 
 
 def run_case(name: str, repeat: int = 3):
@@ -605,6 +605,8 @@ def run_case(name: str, repeat: int = 3):
       sir_field                                      dreamrect, the reference bench_dreamrect element on a
                                                      16x16x32 subset of its field
       sir_arr                                        dream_arr_rect, the reference's array example (arr_example)
+      conv_fmc                                       fmc_synthesis of the TFM test: 101 x 101 double paths of
+                                                     2000-sample SIRs, then the 150-sample pulse (two launches)
     Prints one JSON line with the mean wall time per call (not a bench value)."""
     import torch
     from dream_b200 import das, das_f, synth
@@ -676,6 +678,13 @@ def run_case(name: str, repeat: int = 3):
         Ro = np.stack([X.ravel(order="F"), Yg.ravel(order="F"), Z.ravel(order="F")], 1)
         Rd = torch.from_numpy(np.ascontiguousarray(Ro.T)).to(dev).t()
         fn = lambda: dreamrect(Rd, [10.0, 15.0], [0.05, 0.05, 0.25, 300], 0.0, [1.0, 1000.0, 0.0], "stop")
+    elif name == "conv_fmc":
+        from dream_b200.conv import fmc_synthesis
+        rng = np.random.default_rng(21)
+        Hd = torch.from_numpy(np.ascontiguousarray(rng.normal(size=(101, 2000)))).to(dev).t()
+        tp = np.arange(150) / 50.0
+        pulse = torch.from_numpy(-np.exp(-10.0 * (tp - 0.55) ** 2) * np.cos(2 * np.pi * 2.5 * tp)).to(dev)
+        fn = lambda: fmc_synthesis(Hd, pulse)
     elif name == "sir_arr":
         from dream_b200.dreamrect import dream_arr_rect
         arr = arr_example()
