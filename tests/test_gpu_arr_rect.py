@@ -183,3 +183,21 @@ def test_random_arrays_match_oracle(seed):
     H = _call(c)
     assert np.array_equal(H, ref, equal_nan=True), f"{np.sum(H != ref)} samples differ"
     assert _counts(c, "warn") == _oracle(c, "warn")[1:]
+
+
+def test_full_size_velocity_doubling_is_exact():
+    # the reference's array example at full size (examples/rect_arr_example.m: 21 x 21 elements, 64722
+    # points): doubling v doubles every term exactly, the indices do not depend on v, so H doubles bit for bit
+    from dream_b200.dream_arr_rect import dream_arr_rect
+    x = np.arange(-10.0, 11.0)
+    gx, gy = np.meshgrid(x, x)
+    G = np.asfortranarray(np.stack([gx.ravel(order="F"), gy.ravel(order="F"), np.zeros(gx.size)], 1))
+    X, Z = np.meshgrid(np.arange(-50.0, 50.25, 0.5), np.arange(0.0, 80.25, 0.5))
+    xz = np.stack([X.ravel(order="F"), np.zeros(X.size), Z.ravel(order="F")], 1)
+    Ro = np.concatenate([xz, xz[:, [1, 0, 2]]])
+    Rd = torch.from_numpy(np.ascontiguousarray(Ro.T)).cuda().t()
+    run = lambda v: dream_arr_rect(Rd, [0.9, 0.9], G, [0.03, 0.03, 0.1, 13], 49.0 * 1e3 / 1500.0, [v, 1500.0, 0.0],
+                                   "xy", 50.0, "x", [-25.0, 0.0], "off", np.ones(G.shape[0]), 1.0, "ignore")
+    H1, H2 = run(1.0), run(2.0)
+    assert H1.shape == (13, 64722) and bool(H1.abs().sum() > 0)
+    assert torch.equal(H2, 2 * H1)

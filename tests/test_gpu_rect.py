@@ -84,3 +84,17 @@ def test_random_elements_match_oracle(seed):
     d = np.full((1, 1), rng.uniform(-3, 10)) if rng.random() < 0.6 else rng.uniform(-3, 10, (20, 1))
     ref, _, _ = oracle.rect(c["Ro"], c["a"], c["b"], c["dx"], c["dy"], c["dt"], c["nt"], d, c["v"], c["cp"], "ignore")
     assert np.array_equal(_call(c, delay=d), ref)
+
+
+def test_full_size_velocity_doubling_is_exact():
+    # a 61 x 61 x 32 slab of the reference's bench_dreamrect field (python/tests/bench_dreamrect.py):
+    # doubling v doubles every term exactly and leaves the indices alone, so H doubles bit for bit
+    from dream_b200.dreamrect import dreamrect
+    X, Yg, Z = np.meshgrid(np.linspace(-15, 15, 61), np.linspace(-15, 15, 61), np.linspace(1.25, 65, 256)[::8],
+                           indexing="ij")
+    Ro = np.stack([X.ravel(order="F"), Yg.ravel(order="F"), Z.ravel(order="F")], 1)
+    Rd = torch.from_numpy(np.ascontiguousarray(Ro.T)).cuda().t()
+    run = lambda v: dreamrect(Rd, [10.0, 15.0], [0.05, 0.05, 0.25, 300], 0.0, [v, 1000.0, 0.0], "stop")
+    H1, H2 = run(1.0), run(2.0)
+    assert bool(H1.abs().sum() > 0)
+    assert torch.equal(H2, 2 * H1)
