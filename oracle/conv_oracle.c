@@ -6,10 +6,10 @@
  * TEST INFRASTRUCTURE ONLY: the checker for dream_b200/csrc/conv_p.cu; only
  * tests/ and bench.py's CPU-baseline leg load it.
  *
- * PARITY UNPINNED. The reference's conv.cc and fftconv.cc include fft.h,
- * which needs FFTW's headers; FFTW is not installed here, so neither can be
- * built and run, and the reference's tests hold no stored convolution
- * outputs. This file restates the direct form line for line instead:
+ * Pinned against the reference's own conv() (extra_src/conv.cc, compiled
+ * unmodified by oracle/build_ref.sh into oracle/_ref/libref_cpu.so; stored
+ * outputs in tests/golden/ref_cpu_golden.npz). This file restates the direct
+ * form line for line:
  *   conv()          extra_src/conv.cc:34-78  (zr[i+j] += xr[i]*yr[j], i outer,
  *                   j inner; '=' clears first, '+=' adds, '-=' subtracts)
  *   column loop     extra_src/oct_conv_p.cc:88-96 (column n of A with column n
@@ -17,8 +17,8 @@
  *   argument rules  extra_src/oct_conv_p.cc:225-236, python/include/py_fftconv_p.hpp:70-77
  * fftconv_p (extra_src/fftconv_p.cc, fftconv.cc) computes the same full linear
  * convolution through FFTW, which differs from the direct form by rounding
- * only; the tests compare both against numpy.convolve as an independent
- * implementation.
+ * only (FFTW is not installed here); the tests also compare the direct form
+ * with numpy.convolve as an independent implementation.
  *
  * Compile with -ffp-contract=off: each product and each sum rounds as written.
  */

@@ -188,7 +188,8 @@ CONV_MODES = {"=": 0, "+=": 1, "-=": 2}
 
 def conv_p(A, B, Y=None, mode="="):
     """Column-wise full linear convolution, the direct form of the reference's
-    conv() (conv_oracle.c; parity unpinned: the reference needs FFTW to build).
+    conv() (conv_oracle.c; pinned against the reference's own conv(), see
+    reference_conv_p).
     Returns Y ((A_M + B_M - 1) x A_N, FP64, column-major); with Y given it is
     updated in place by mode '=', '+=' or '-='."""
     A = np.asfortranarray(np.asarray(A, dtype=np.float64))
@@ -224,7 +225,7 @@ def rect(Ro, a, b, dx, dy, dt, nt, delay, v, cp, err_level="ignore"):
 
 def reference_rect(Ro, a, b, dx, dy, dt, nt, delay, v, cp):
     """The reference's OpenCL dreamrect kernel compiled as C (oracle/_ref,
-    built by build_ref.sh from /root/reference), or None when absent."""
+    built by build_ref.sh from the reference sources), or None when absent."""
     path = os.path.join(REF_DIR, "libref_dreamrect.so")
     if not os.path.exists(path):
         return None
@@ -289,3 +290,97 @@ def arr_rect(Ro, a, b, G, dx, dy, dt, nt, delay, v, cp, foc_met="off", focal=0.0
                                      float(theta), float(phi), APOD_METHODS[apod_met], _p(apod), float(apod_par),
                                      ERR_LEVELS[err_level], _p(H), ctypes.byref(oob))
     return H, st, oob.value
+
+# ---------------------------------------------------------------------------
+# The reference's own CPU code (oracle/_ref/libref_cpu.so, built unmodified by
+# build_ref.sh with FFTW replaced by oracle/fftw_stub.c): conv() of
+# extra_src/conv.cc, Rect::dreamrect of src/dreamrect.cc and
+# ArrRect::dream_arr_rect of src/dream_arr_rect.cc, without attenuation.
+# Each returns None when the library is absent.
+# ---------------------------------------------------------------------------
+
+_ref_cpu = None
+
+
+def reference_cpu():
+    global _ref_cpu
+    if _ref_cpu is None:
+        path = os.path.join(REF_DIR, "libref_cpu.so")
+        if not os.path.exists(path):
+            return None
+        L = ctypes.CDLL(path)
+        vp, i64, f64, i32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_int
+        L.dream_ref_conv.argtypes = [vp, i64, vp, i64, vp, i32]
+        L.dream_ref_conv.restype = None
+        L.dream_ref_dreamrect.argtypes = [vp, i64, f64, f64, f64, f64, f64, i64, i32, vp, f64, f64, i32, vp]
+        L.dream_ref_dreamrect.restype = i32
+        L.dream_ref_arr_rect.argtypes = [vp, i64, f64, f64, f64, f64, f64, i64, i32, vp, f64, f64, i64, vp, i32, vp,
+                                         i32, f64, f64, i32, vp, f64, i32, vp]
+        L.dream_ref_arr_rect.restype = i32
+        _ref_cpu = L
+    return _ref_cpu
+
+
+CONV_MODES = {"=": 0, "+=": 1, "-=": 2}
+
+
+def reference_conv_p(A, B, Y=None, mode="="):
+    """Column-wise conv() of the reference (extra_src/conv.cc:33-78) as
+    conv_p calls it: column n of A convolved with column n of B (or with the
+    single column B); ``Y`` is updated in place for '+=' / '-='."""
+    L = reference_cpu()
+    if L is None:
+        return None
+    A = np.asfortranarray(np.asarray(A, dtype=np.float64))
+    B = np.asfortranarray(np.asarray(B, dtype=np.float64))
+    if A.ndim == 1:
+        A = A.reshape(-1, 1, order="F")
+    if B.ndim == 1:
+        B = B.reshape(-1, 1, order="F")
+    M, N = A.shape
+    Lb, nb = B.shape
+    if Y is None:
+        Y = np.zeros((M + Lb - 1, N), order="F")
+    else:
+        Y = np.asfortranarray(np.array(Y, dtype=np.float64))
+    for n in range(N):
+        a = np.ascontiguousarray(A[:, n])
+        b = np.ascontiguousarray(B[:, n if nb > 1 else 0])
+        y = np.ascontiguousarray(Y[:, n])
+        L.dream_ref_conv(_p(a), M, _p(b), Lb, _p(y), CONV_MODES[mode])
+        Y[:, n] = y
+    return Y
+
+
+def reference_dreamrect(Ro, a, b, dx, dy, dt, nt, delay, v, cp, err_level="ignore"):
+    """The reference's CPU dreamrect: ``(H, status)``, H nt x No."""
+    L = reference_cpu()
+    if L is None:
+        return None
+    Ro = np.asfortranarray(np.asarray(Ro, dtype=np.float64))
+    delay = np.ascontiguousarray(np.asarray(delay, dtype=np.float64).reshape(-1))
+    H = np.zeros((int(nt), Ro.shape[0]), dtype=np.float64, order="F")
+    st = L.dream_ref_dreamrect(_p(Ro), Ro.shape[0], a, b, dx, dy, dt, int(nt), int(delay.size > 1), _p(delay), v, cp,
+                               ERR_LEVELS[err_level], _p(H))
+    return H, st
+
+
+def reference_arr_rect(Ro, a, b, G, dx, dy, dt, nt, delay, v, cp, foc_met="off", focal=0.0, steer_met="off",
+                       theta=0.0, phi=0.0, apod_met="off", apod=None, apod_par=0.0, err_level="ignore"):
+    """The reference's CPU dream_arr_rect (arguments as arr_rect): ``(H, status)``."""
+    L = reference_cpu()
+    if L is None:
+        return None
+    Ro = np.asfortranarray(np.asarray(Ro, dtype=np.float64))
+    G, focal, apod = _arr_args(G, focal, apod)
+    if apod is None:
+        apod = np.ones(G.shape[0])
+    if focal.size < G.shape[0]:
+        focal = np.resize(focal, G.shape[0])  # the reference reads focal[n] for 'ud' only
+    delay = np.ascontiguousarray(np.asarray(delay, dtype=np.float64).reshape(-1))
+    H = np.zeros((int(nt), Ro.shape[0]), dtype=np.float64, order="F")
+    st = L.dream_ref_arr_rect(_p(Ro), Ro.shape[0], a, b, dx, dy, dt, int(nt), int(delay.size > 1), _p(delay), v, cp,
+                              G.shape[0], _p(G), FOC_METHODS[foc_met], _p(focal), STEER_METHODS[steer_met],
+                              float(theta), float(phi), APOD_METHODS[apod_met], _p(apod), float(apod_par),
+                              ERR_LEVELS[err_level], _p(H))
+    return H, st

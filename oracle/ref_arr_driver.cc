@@ -9,43 +9,11 @@
 #include <stdint.h>
 
 #include "arr_functions.h"
+#include "ref_enums.h"
 
-namespace {
-
-FocusMet foc_of(int m) {
-  switch (m) {
-    case 1: return FocusMet::x;
-    case 2: return FocusMet::y;
-    case 3: return FocusMet::xy;
-    case 4: return FocusMet::x_y;
-    case 5: return FocusMet::ud;
-    default: return FocusMet::none;
-  }
-}
-
-SteerMet steer_of(int m) {
-  switch (m) {
-    case 1: return SteerMet::x;
-    case 2: return SteerMet::y;
-    case 3: return SteerMet::xy;
-    default: return SteerMet::none;
-  }
-}
-
-ApodMet apod_of(int m) {
-  switch (m) {
-    case 1: return ApodMet::triangle;
-    case 2: return ApodMet::gauss;
-    case 3: return ApodMet::raised_cosine;
-    case 4: return ApodMet::hann;
-    case 5: return ApodMet::hamming;
-    case 6: return ApodMet::simply_supported;
-    case 7: return ApodMet::clamped;
-    default: return ApodMet::ud;
-  }
-}
-
-}  // namespace
+using ref_codes::apod_of;
+using ref_codes::foc_of;
+using ref_codes::steer_of;
 
 extern "C" void dream_ref_arr_elements(double *G, int64_t M, int foc_met, double *focal, int steer_met,
                                        double theta, double phi, int apod_met, double *apod, double apod_par,

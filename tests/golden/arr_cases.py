@@ -80,3 +80,30 @@ ARR_CASES = {
                            np.array([[0.0, 0.0, 0.0], [0.02, 0.01, 0.0]]), 0.01, 0.01, 1e-6, 6000,
                            1000.0 * 1e3 / 1500.0),
 }
+
+# method names accepted by dream_arr_rect (the keys of oracle.FOC_METHODS, ...)
+FOC_NAMES = ["off", "x", "y", "xy", "on", "x+y", "ud"]
+STEER_NAMES = ["off", "x", "y", "xy"]
+APOD_NAMES = ["off", "triangle", "gauss", "raised", "hann", "hamming", "simply", "clamped", "ud"]
+
+
+def random_case(seed):
+    """A seeded random array, sampling and method choice (small enough for the oracle)."""
+    rng = np.random.default_rng(seed)
+    M = int(rng.integers(1, 40))
+    a, b = rng.uniform(0.05, 2.0, 2)
+    dx, dy = a / rng.integers(1, 40), b / rng.integers(1, 40)
+    G = np.asfortranarray(np.stack([rng.uniform(-6, 6, M), rng.uniform(-6, 6, M), rng.uniform(-0.5, 0.5, M)], 1))
+    No = int(rng.integers(1, 24))
+    Ro = np.asfortranarray(np.stack([rng.uniform(-10, 10, No), rng.uniform(-10, 10, No), rng.uniform(0.2, 25, No)], 1))
+    cp = float(rng.uniform(1000, 6000))
+    dt = float(rng.choice([0.005, 0.02, 0.1, 0.25]))
+    nt = int(rng.integers(1, 2500))
+    delay = float(rng.uniform(-2, 8)) if rng.random() < 0.7 else rng.uniform(-2, 8, No)
+    foc = str(rng.choice(list(FOC_NAMES)))
+    steer = str(rng.choice(list(STEER_NAMES)))
+    apod = str(rng.choice(list(APOD_NAMES)))
+    return dict(Ro=Ro, a=a, b=b, G=G, dx=dx, dy=dy, dt=dt, nt=nt, delay=delay, v=float(rng.uniform(0.5, 2)), cp=cp,
+                foc_met=foc, focal=rng.uniform(0, 1, M) if foc == "ud" else float(rng.uniform(2, 30)),
+                steer_met=steer, theta=float(rng.uniform(-40, 40)), phi=float(rng.uniform(-40, 40)),
+                apod_met=apod, apod=rng.uniform(0.1, 1.5, M) if apod == "ud" else None, apod_par=0.0, err="ignore")

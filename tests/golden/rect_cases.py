@@ -32,3 +32,16 @@ RECT_CASES = {
     "neg_delay": dict(Ro=_cloud(4, 12, (-3, 3), (-3, 3), (5, 15)), a=1.3, b=0.7, dx=0.013, dy=0.021, dt=0.02,
                       nt=900, delay=-0.4, v=1.0, cp=1540.0),
 }
+
+
+def random_rect_case(seed):
+    """A seeded random element, discretisation, sampling and 20 points, with one
+    delay or one per point: returns (case, delay)."""
+    rng = np.random.default_rng(100 + seed)
+    a, b = rng.uniform(0.05, 12.0, 2)
+    c = dict(Ro=np.asfortranarray(np.stack([rng.uniform(-15, 15, 20), rng.uniform(-15, 15, 20),
+                                            rng.uniform(0.1, 40, 20)], 1)),
+             a=a, b=b, dx=a / rng.integers(1, 120), dy=b / rng.integers(1, 120), dt=float(rng.choice([0.01, 0.05, 0.25])),
+             nt=int(rng.integers(1, 3000)), v=float(rng.uniform(0.5, 2)), cp=float(rng.uniform(1000, 6000)))
+    d = np.full((1, 1), rng.uniform(-3, 10)) if rng.random() < 0.6 else rng.uniform(-3, 10, (20, 1))
+    return c, d

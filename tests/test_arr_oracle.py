@@ -1,15 +1,19 @@
 """dream_arr_rect oracle (oracle/rect_oracle.c) pinned against the reference:
-per-element focusing / steering / apodisation against src/arr_functions.cc
-(compiled unmodified; tests/golden/arr_golden.npz), one-element arrays
-against the reference's dreamrect kernel (opencl/dreamrect.cl), the
-last-element status rule of src/dream_arr_rect.cc:209-243, and the front
-end's argument checks (no GPU)."""
+the whole element summation against the reference's CPU dream_arr_rect
+(src/dream_arr_rect.cc, compiled unmodified into oracle/_ref/libref_cpu.so:
+every case of arr_cases.py in tests/golden/ref_cpu_golden.npz, and the live
+library on 40 seeded random arrays); per-element focusing / steering /
+apodisation against src/arr_functions.cc (compiled unmodified;
+tests/golden/arr_golden.npz), one-element arrays against the reference's
+dreamrect kernel (opencl/dreamrect.cl), the last-element status rule of
+src/dream_arr_rect.cc:209-243, and the front end's argument checks (no GPU)."""
 import os
 
 import numpy as np
 import pytest
 
-from arr_cases import ARR_CASES
+from arr_cases import ARR_CASES, random_case
+from gen_cpu_golden import arr_args, arr_kw
 from gen_arr_golden import (APOD_PAR, APOD_UD, CP, FOCAL_UD, G7, ONE_ELEMENT, PHI, THETA,
                             one_element_points)
 from oracle import oracle
@@ -18,6 +22,34 @@ from oracle import oracle
 @pytest.fixture(scope="module")
 def golden():
     return np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "arr_golden.npz"))
+
+
+@pytest.fixture(scope="module")
+def cpu_golden():
+    return np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_cpu_golden.npz"))
+
+
+@pytest.mark.parametrize("name", sorted(ARR_CASES))
+def test_oracle_matches_reference_cpu_arr_rect(name, cpu_golden):
+    c = ARR_CASES[name]
+    H, st, oob = oracle.arr_rect(*arr_args(c), **arr_kw(c))
+    assert np.array_equal(H, cpu_golden[f"arr|{name}"], equal_nan=True)
+    assert st == int(cpu_golden[f"arr_st|{name}"])
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_oracle_matches_live_reference_cpu_arr_rect(seed):
+    if oracle.reference_cpu() is None:
+        pytest.skip("oracle/_ref/libref_cpu.so not built")
+    c = dict(random_case(seed), err="warn")
+    H, st, _ = oracle.arr_rect(*arr_args(c), **arr_kw(c))
+    R, st_ref = oracle.reference_arr_rect(*arr_args(c), **arr_kw(c))
+    assert np.array_equal(H, R, equal_nan=True)
+    # The reference reads the threads' statuses only when it ran more than one
+    # thread (src/dream_arr_rect.cc:415-424); a single-threaded run returns
+    # SIRError::none whatever its points reported.
+    threads = min(os.cpu_count() or 1, c["Ro"].shape[0], int(os.environ.get("DREAM_NUM_THREADS", 1 << 30)))
+    assert st == st_ref if threads > 1 else st_ref == 0
 
 
 COMBOS = [(f, s, a) for f in oracle.FOC_METHODS for s in oracle.STEER_METHODS for a in oracle.APOD_METHODS]

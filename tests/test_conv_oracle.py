@@ -1,11 +1,45 @@
 """The convolution restatement (oracle/conv_oracle.c, direct form of the
-reference's conv()) against numpy.convolve, an independent implementation,
-and the front end's argument rules; no GPU. Parity with the reference itself
-is unpinned: its conv.cc / fftconv.cc need FFTW's headers to build."""
+reference's conv()) pinned against the reference's own conv()
+(extra_src/conv.cc, compiled unmodified into oracle/_ref/libref_cpu.so):
+stored outputs in tests/golden/ref_cpu_golden.npz (gen_cpu_golden.py) and the
+live library when built; also against numpy.convolve, an independent
+implementation, and the front end's argument rules; no GPU."""
+import os
+
 import numpy as np
 import pytest
 
+from gen_cpu_golden import CONV_CASES, conv_inputs
 from oracle import oracle
+
+
+@pytest.fixture(scope="module")
+def cpu_golden():
+    return np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_cpu_golden.npz"))
+
+
+@pytest.mark.parametrize("mode", ["=", "+=", "-="])
+@pytest.mark.parametrize("name", sorted(CONV_CASES))
+def test_oracle_matches_reference_conv(name, mode, cpu_golden):
+    A, B, Y0 = conv_inputs(name)
+    Y = oracle.conv_p(A, B, None if mode == "=" else Y0.copy(order="F"), mode)
+    assert np.array_equal(Y, cpu_golden[f"conv|{name}|{mode}"])
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_oracle_matches_live_reference_conv(seed):
+    if oracle.reference_cpu() is None:
+        pytest.skip("oracle/_ref/libref_cpu.so not built")
+    rng = np.random.default_rng(50 + seed)
+    A_M, A_N, B_M = (int(v) for v in rng.integers(1, 400, 3))
+    A_N = A_N % 6 + 1
+    B = rng.normal(size=(B_M, A_N if seed % 2 else 1))
+    A = rng.normal(size=(A_M, A_N))
+    Y0 = np.asfortranarray(rng.normal(size=(A_M + B_M - 1, A_N)))
+    for mode in ("=", "+=", "-="):
+        y0 = None if mode == "=" else Y0
+        ref = oracle.reference_conv_p(A, B, y0, mode)
+        assert np.array_equal(oracle.conv_p(A, B, None if y0 is None else y0.copy(order="F"), mode), ref)
 
 
 def np_conv(A, B):

@@ -10,7 +10,7 @@ import os
 import numpy as np
 import pytest
 
-from arr_cases import ARR_CASES
+from arr_cases import ARR_CASES, random_case
 from gen_arr_golden import ONE_ELEMENT, one_element_points
 from oracle import oracle
 
@@ -154,50 +154,39 @@ def test_host_exception_becomes_a_status():
     assert L.dream_das_last_error()
 
 
-def _random_case(seed):
-    """A seeded random array, sampling and method choice (small enough for the oracle)."""
-    rng = np.random.default_rng(seed)
-    M = int(rng.integers(1, 40))
-    a, b = rng.uniform(0.05, 2.0, 2)
-    dx, dy = a / rng.integers(1, 40), b / rng.integers(1, 40)
-    G = np.asfortranarray(np.stack([rng.uniform(-6, 6, M), rng.uniform(-6, 6, M), rng.uniform(-0.5, 0.5, M)], 1))
-    No = int(rng.integers(1, 24))
-    Ro = np.asfortranarray(np.stack([rng.uniform(-10, 10, No), rng.uniform(-10, 10, No), rng.uniform(0.2, 25, No)], 1))
-    cp = float(rng.uniform(1000, 6000))
-    dt = float(rng.choice([0.005, 0.02, 0.1, 0.25]))
-    nt = int(rng.integers(1, 2500))
-    delay = float(rng.uniform(-2, 8)) if rng.random() < 0.7 else rng.uniform(-2, 8, No)
-    foc = str(rng.choice(list(oracle.FOC_METHODS)))
-    steer = str(rng.choice(list(oracle.STEER_METHODS)))
-    apod = str(rng.choice(list(oracle.APOD_METHODS)))
-    return dict(Ro=Ro, a=a, b=b, G=G, dx=dx, dy=dy, dt=dt, nt=nt, delay=delay, v=float(rng.uniform(0.5, 2)), cp=cp,
-                foc_met=foc, focal=rng.uniform(0, 1, M) if foc == "ud" else float(rng.uniform(2, 30)),
-                steer_met=steer, theta=float(rng.uniform(-40, 40)), phi=float(rng.uniform(-40, 40)),
-                apod_met=apod, apod=rng.uniform(0.1, 1.5, M) if apod == "ud" else None, apod_par=0.0, err="ignore")
-
-
 @pytest.mark.parametrize("seed", range(40))
 def test_random_arrays_match_oracle(seed):
-    c = _random_case(seed)
+    c = random_case(seed)
     ref, st_ref, oob_ref = _oracle(c)
     H = _call(c)
     assert np.array_equal(H, ref, equal_nan=True), f"{np.sum(H != ref)} samples differ"
     assert _counts(c, "warn") == _oracle(c, "warn")[1:]
 
 
-def test_full_size_velocity_doubling_is_exact():
-    # the reference's array example at full size (examples/rect_arr_example.m: 21 x 21 elements, 64722
-    # points): doubling v doubles every term exactly, the indices do not depend on v, so H doubles bit for bit
+def test_full_size_array_example_matches_reference():
+    """The reference's array example at full size (examples/rect_arr_example.m:
+    21 x 21 elements of 0.9 x 0.9 mm, xy focusing at 50 mm, steering -25 deg,
+    64722 points on two planes, a 13-sample window) against the reference's own
+    CPU dream_arr_rect (oracle/_ref/libref_cpu.so; the C restatement when that
+    library is absent), bit for bit, plus the exact scaling in v."""
     from dream_b200.dream_arr_rect import dream_arr_rect
     x = np.arange(-10.0, 11.0)
     gx, gy = np.meshgrid(x, x)
     G = np.asfortranarray(np.stack([gx.ravel(order="F"), gy.ravel(order="F"), np.zeros(gx.size)], 1))
     X, Z = np.meshgrid(np.arange(-50.0, 50.25, 0.5), np.arange(0.0, 80.25, 0.5))
     xz = np.stack([X.ravel(order="F"), np.zeros(X.size), Z.ravel(order="F")], 1)
-    Ro = np.concatenate([xz, xz[:, [1, 0, 2]]])
+    Ro = np.asfortranarray(np.concatenate([xz, xz[:, [1, 0, 2]]]))
+    delay = 49.0 * 1e3 / 1500.0
+    args = (Ro, 0.9, 0.9, G, 0.03, 0.03, 0.1, 13, delay, 1.0, 1500.0)
+    kw = dict(foc_met="xy", focal=50.0, steer_met="x", theta=-25.0, phi=0.0, apod_met="off", apod=None,
+              apod_par=0.0, err_level="ignore")
+    ref = oracle.reference_arr_rect(*args, **kw)
+    ref = ref[0] if ref is not None else oracle.arr_rect(*args, **kw)[0]
     Rd = torch.from_numpy(np.ascontiguousarray(Ro.T)).cuda().t()
-    run = lambda v: dream_arr_rect(Rd, [0.9, 0.9], G, [0.03, 0.03, 0.1, 13], 49.0 * 1e3 / 1500.0, [v, 1500.0, 0.0],
-                                   "xy", 50.0, "x", [-25.0, 0.0], "off", np.ones(G.shape[0]), 1.0, "ignore")
-    H1, H2 = run(1.0), run(2.0)
+    run = lambda v: dream_arr_rect(Rd, [0.9, 0.9], G, [0.03, 0.03, 0.1, 13], delay, [v, 1500.0, 0.0], "xy", 50.0,
+                                   "x", [-25.0, 0.0], "off", np.ones(G.shape[0]), 1.0, "ignore")
+    H1 = run(1.0)
     assert H1.shape == (13, 64722) and bool(H1.abs().sum() > 0)
-    assert torch.equal(H2, 2 * H1)
+    H = H1.cpu().numpy()
+    assert np.array_equal(H, ref), f"{np.sum(H != ref)} of {H.size} samples differ"
+    assert torch.equal(run(2.0), 2 * H1)

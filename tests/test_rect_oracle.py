@@ -1,12 +1,40 @@
-"""dreamrect oracle (oracle/rect_oracle.c) pinned against the reference:
-its OpenCL kernel opencl/dreamrect.cl compiled unmodified as C
-(tests/golden/rect_golden.npz, generated by tests/golden/gen_rect_golden.py);
-error levels; the front end's argument checks (no GPU)."""
+"""dreamrect oracle (oracle/rect_oracle.c) pinned against the reference
+twice: its OpenCL kernel opencl/dreamrect.cl compiled unmodified as C
+(tests/golden/rect_golden.npz, generated by tests/golden/gen_rect_golden.py),
+and its CPU dreamrect (src/dreamrect.cc, compiled unmodified into
+oracle/_ref/libref_cpu.so; tests/golden/ref_cpu_golden.npz and the live
+library on seeded random elements); error levels; the front end's argument
+checks (no GPU)."""
+import os
+
 import numpy as np
 import pytest
 
 from oracle import oracle
-from rect_cases import RECT_CASES
+from rect_cases import RECT_CASES, random_rect_case
+
+
+@pytest.fixture(scope="module")
+def cpu_golden():
+    return np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_cpu_golden.npz"))
+
+
+@pytest.mark.parametrize("name", sorted(RECT_CASES))
+def test_oracle_matches_reference_cpu_dreamrect(name, cpu_golden):
+    H, st, oob = _run(RECT_CASES[name])
+    assert np.array_equal(H, cpu_golden[f"rect|{name}"])
+    assert st == int(cpu_golden[f"rect_st|{name}"])
+
+
+@pytest.mark.parametrize("seed", range(24))
+def test_oracle_matches_live_reference_cpu_dreamrect(seed):
+    if oracle.reference_cpu() is None:
+        pytest.skip("oracle/_ref/libref_cpu.so not built")
+    c, d = random_rect_case(seed)
+    args = (c["Ro"], c["a"], c["b"], c["dx"], c["dy"], c["dt"], c["nt"], d, c["v"], c["cp"])
+    H, st, _ = oracle.rect(*args, "warn")
+    R, st_ref = oracle.reference_dreamrect(*args, "warn")
+    assert np.array_equal(H, R) and st == st_ref
 
 
 @pytest.fixture(scope="module")
