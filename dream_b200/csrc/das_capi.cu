@@ -747,6 +747,59 @@ int dream_das_op_backward(dream_das_plan *p, const float *dG, const float *dY, c
 
 }  // extern "C"
 
+namespace dream {
+// One batch frame: validated and turned into its launch descriptor (oob
+// pointer left NULL). Shared by dream_das_batch_create and the allocation-free
+// batch entry so that both accept exactly the same frames.
+int batch_frame_params(const dream_das_frame &d, FastParams &F) {
+  int r = check_common(d.das_type, d.a_scan_len, d.No, d.num_t_elements, d.num_r_elements, DREAM_PREC_F32_STORE);
+  if (!r && (d.das_type == DREAM_DAS_SAFT || d.num_r_elements == 0))
+    r = fail(DREAM_ERR_UNSUPPORTED, "batch frames must be TFM or RCA");
+  if (!r && d.das_type >= DREAM_DAS_RCA_COLTX) r = check_rca_edges(d.num_t_elements, d.num_r_elements);
+  if (!r && (d.n_fast < 0 || (d.n_fast > 0 && d.No % d.n_fast)))
+    r = fail(DREAM_ERR_ARGUMENT, "grid hint must divide the number of image points");
+  if (!r && (d.tile_f || d.tile_s) &&
+      (d.tile_f * d.tile_s != 128 || (d.n_fast > 0 ? (d.tile_f % 8 || d.tile_s % 4) : d.tile_s != 1)))
+    r = fail(DREAM_ERR_ARGUMENT, "invalid frame tile (tile_f * tile_s must be 128)");
+  if (!r && d.jc != 0 && d.jc != 8 && d.jc != 16) r = fail(DREAM_ERR_ARGUMENT, "chunk must be 0, 8 or 16");
+  if (!r && d.No > 0 && d.a_scan_len > 0 &&
+      (d.Y == nullptr || d.Ro == nullptr || d.Gt == nullptr || d.Gr == nullptr || d.delay == nullptr || d.Im == nullptr))
+    r = fail(DREAM_ERR_ARGUMENT, "NULL frame pointer");
+  if (r) return r;
+  memset(&F, 0, sizeof(F));
+  F.method = d.das_type;
+  F.Y = d.Y;
+  F.K = d.a_scan_len;
+  F.Ro = d.Ro;
+  F.No = d.No;
+  F.Gt = d.Gt;
+  F.Nt = (int)d.num_t_elements;
+  F.Gr = d.Gr;
+  F.Nr = (int)d.num_r_elements;
+  F.delay = d.delay;
+  F.delay_multi = d.delay_type == DREAM_DELAY_MULTIPLE;
+  Consts64 c = constants_f64(d.dt, d.cp, 0.0);
+  F.Fs = c.Fs;
+  F.ocp = c.ocp;
+  F.Im = d.Im;
+  if (d.n_fast > 0) {
+    F.n_fast = d.n_fast;
+    F.n_slow = d.No / d.n_fast;
+    F.wf = 8;
+    F.tile_f = d.tile_f ? d.tile_f : 16;
+    F.tile_s = d.tile_s ? d.tile_s : 8;
+  } else {
+    F.n_fast = d.No;
+    F.n_slow = 1;
+    F.wf = 32;
+    F.tile_f = 128;
+    F.tile_s = 1;
+  }
+  F.jc = d.jc ? d.jc : 16;
+  return 0;
+}
+}  // namespace dream
+
 struct dream_das_batch {
   int device = 0;
   bool bf16 = false;
@@ -785,54 +838,12 @@ int dream_das_batch_create(dream_das_batch **out, const dream_das_frame *fr, int
   std::vector<Group> groups;
   for (int f = 0; f < n_frames; f++) {
     const dream_das_frame &d = fr[f];
-    int r = check_common(d.das_type, d.a_scan_len, d.No, d.num_t_elements, d.num_r_elements, DREAM_PREC_F32_STORE);
-    if (!r && (d.das_type == DREAM_DAS_SAFT || d.num_r_elements == 0))
-      r = fail(DREAM_ERR_UNSUPPORTED, "batch frames must be TFM or RCA");
-    if (!r && d.das_type >= DREAM_DAS_RCA_COLTX) r = check_rca_edges(d.num_t_elements, d.num_r_elements);
-    if (!r && (d.n_fast < 0 || (d.n_fast > 0 && d.No % d.n_fast)))
-      r = fail(DREAM_ERR_ARGUMENT, "grid hint must divide the number of image points");
-    if (!r && (d.tile_f || d.tile_s) &&
-        (d.tile_f * d.tile_s != 128 || (d.n_fast > 0 ? (d.tile_f % 8 || d.tile_s % 4) : d.tile_s != 1)))
-      r = fail(DREAM_ERR_ARGUMENT, "invalid frame tile (tile_f * tile_s must be 128)");
-    if (!r && d.jc != 0 && d.jc != 8 && d.jc != 16) r = fail(DREAM_ERR_ARGUMENT, "chunk must be 0, 8 or 16");
-    if (!r && d.No > 0 && d.a_scan_len > 0 &&
-        (d.Y == nullptr || d.Ro == nullptr || d.Gt == nullptr || d.Gr == nullptr || d.delay == nullptr || d.Im == nullptr))
-      r = fail(DREAM_ERR_ARGUMENT, "NULL frame pointer");
+    FastParams F;
+    int r = batch_frame_params(d, F);
     if (r) {
       dream_das_batch_destroy(b);
       return r;
     }
-    FastParams F;
-    memset(&F, 0, sizeof(F));
-    F.method = d.das_type;
-    F.Y = d.Y;
-    F.K = d.a_scan_len;
-    F.Ro = d.Ro;
-    F.No = d.No;
-    F.Gt = d.Gt;
-    F.Nt = (int)d.num_t_elements;
-    F.Gr = d.Gr;
-    F.Nr = (int)d.num_r_elements;
-    F.delay = d.delay;
-    F.delay_multi = d.delay_type == DREAM_DELAY_MULTIPLE;
-    Consts64 c = constants_f64(d.dt, d.cp, 0.0);
-    F.Fs = c.Fs;
-    F.ocp = c.ocp;
-    F.Im = d.Im;
-    if (d.n_fast > 0) {
-      F.n_fast = d.n_fast;
-      F.n_slow = d.No / d.n_fast;
-      F.wf = 8;
-      F.tile_f = d.tile_f ? d.tile_f : 16;
-      F.tile_s = d.tile_s ? d.tile_s : 8;
-    } else {
-      F.n_fast = d.No;
-      F.n_slow = 1;
-      F.wf = 32;
-      F.tile_f = 128;
-      F.tile_s = 1;
-    }
-    F.jc = d.jc ? d.jc : 16;
     b->smem = std::max(b->smem, fast_smem_bytes(F, 128));
     b->frames.push_back(F);
     if (d.No > 0 && d.a_scan_len > 0) {

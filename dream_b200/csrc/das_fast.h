@@ -32,6 +32,10 @@ struct FastParams {
   // elements) and whether to add into Im instead of writing it
   int in_lo, in_hi;
   int accumulate;
+  // A-scan columns present in Y: column (o, i) is o * ycol_o + i - ycol_i0
+  // (ycol_o == 0: o * n_in + i, the full layout)
+  int64_t ycol_o;
+  int ycol_i0;
   int64_t ny;               // elements in Y (bounds-checked builds; 0: K * columns)
   unsigned long long *bad;  // gather index violations (bounds-checked builds)
 };
@@ -61,4 +65,13 @@ cudaError_t launch_batch(const FastParams *frames, const int4 *items, int n_item
                          int grid, cudaStream_t st);
 int batch_prepare(size_t smem, bool bf16);
 
+}  // namespace dream
+
+struct dream_das_frame;
+
+namespace dream {
+// Validates one batch frame and fills its launch descriptor (oob left NULL);
+// returns 0 or a DREAM_ERR_* status with the message recorded. Used by
+// dream_das_batch_create and dream_das_batch_run_noalloc alike.
+int batch_frame_params(const ::dream_das_frame &d, FastParams &F);
 }  // namespace dream

@@ -69,6 +69,17 @@ extern "C" int dream_das_batch_run_noalloc(const dream_das_frame *fr, int n_fram
   if (e != cudaSuccess) return set_last_error(DREAM_ERR_CUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
   if (device < 0 || device >= ndev || device >= MAX_DEVICES)
     return set_last_error(DREAM_ERR_ARGUMENT, "invalid CUDA device ordinal");
+  // The frame table and tile list are staged in a host array that every call
+  // rewrites, and copied from there on the stream; a graph captured from this
+  // call would re-read that array when replayed. So a stream that is being
+  // captured is refused.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if ((e = cudaStreamIsCapturing((cudaStream_t)stream, &cap)) != cudaSuccess)
+    return set_last_error(DREAM_ERR_CUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e));
+  if (cap != cudaStreamCaptureStatusNone)
+    return set_last_error(DREAM_ERR_UNSUPPORTED,
+                          "dream_das_batch_run_noalloc cannot run on a stream that is being captured: it copies "
+                          "its frame table from a host array that every call rewrites");
   std::lock_guard<std::mutex> lk(g_mu);
   int prev = -1;
   cudaGetDevice(&prev);
@@ -92,55 +103,10 @@ extern "C" int dream_das_batch_run_noalloc(const dream_das_frame *fr, int n_fram
   int *order = reinterpret_cast<int *>(g_host_stage + order_off);
   size_t smem = 1024;
   for (int f = 0; f < n_frames; f++) {
-    const dream_das_frame &d = fr[f];
-    if (d.das_type != DREAM_DAS_TFM && d.das_type != DREAM_DAS_RCA_COLTX && d.das_type != DREAM_DAS_RCA_ROWTX)
-      return set_last_error(DREAM_ERR_UNSUPPORTED, "batch frames must be TFM or RCA");
-    if (d.a_scan_len < 0 || d.No < 0 || d.num_t_elements < 1 || d.num_r_elements < 1 || d.a_scan_len > INT32_MAX ||
-        d.num_t_elements > INT32_MAX || d.num_r_elements > INT32_MAX)
-      return set_last_error(DREAM_ERR_ARGUMENT, "invalid frame size");
-    if (d.das_type != DREAM_DAS_TFM &&
-        (2 * d.num_t_elements - 1 >= 3 * d.num_r_elements || d.num_r_elements - 1 >= 3 * d.num_t_elements))
-      return set_last_error(DREAM_ERR_ARGUMENT, "RCA stripe edges would be read outside Gt/Gr");
-    if (d.n_fast < 0 || (d.n_fast > 0 && d.No % d.n_fast))
-      return set_last_error(DREAM_ERR_ARGUMENT, "grid hint must divide the number of image points");
-    if ((d.tile_f || d.tile_s) &&
-        (d.tile_f * d.tile_s != 128 || (d.n_fast > 0 ? (d.tile_f % 8 || d.tile_s % 4) : d.tile_s != 1)))
-      return set_last_error(DREAM_ERR_ARGUMENT, "invalid frame tile (tile_f * tile_s must be 128)");
-    if (d.jc != 0 && d.jc != 8 && d.jc != 16) return set_last_error(DREAM_ERR_ARGUMENT, "chunk must be 0, 8 or 16");
-    if (d.No > 0 && d.a_scan_len > 0 &&
-        (d.Y == nullptr || d.Ro == nullptr || d.Gt == nullptr || d.Gr == nullptr || d.delay == nullptr || d.Im == nullptr))
-      return set_last_error(DREAM_ERR_ARGUMENT, "NULL frame pointer");
     FastParams &F = T[f];
-    memset(&F, 0, sizeof(F));
-    F.method = d.das_type;
-    F.Y = d.Y;
-    F.K = d.a_scan_len;
-    F.Ro = d.Ro;
-    F.No = d.No;
-    F.Gt = d.Gt;
-    F.Nt = (int)d.num_t_elements;
-    F.Gr = d.Gr;
-    F.Nr = (int)d.num_r_elements;
-    F.delay = d.delay;
-    F.delay_multi = d.delay_type == DREAM_DELAY_MULTIPLE;
-    F.Fs = (1.0 / d.dt) * 1000.0;  // as DAS<double> (extra_src/das.cc:316-317)
-    F.ocp = 1.0 / d.cp;
-    F.Im = d.Im;
+    const int r = batch_frame_params(fr[f], F);
+    if (r) return r;
     F.oob = d_oob;
-    if (d.n_fast > 0) {
-      F.n_fast = d.n_fast;
-      F.n_slow = d.No / d.n_fast;
-      F.wf = 8;
-      F.tile_f = d.tile_f ? d.tile_f : 16;
-      F.tile_s = d.tile_s ? d.tile_s : 8;
-    } else {
-      F.n_fast = d.No;
-      F.n_slow = 1;
-      F.wf = 32;
-      F.tile_f = 128;
-      F.tile_s = 1;
-    }
-    F.jc = d.jc ? d.jc : 16;
     smem = std::max(smem, fast_smem_bytes(F, 128));
     order[f] = f;
   }

@@ -330,10 +330,14 @@ void dream_das_batch_destroy(dream_das_batch *batch);
  * frame table and tile list go to a 4 MiB device array inside this library
  * (every GPU that loads the library holds it until exit). Batches needing
  * more scratch are rejected with DREAM_ERR_ARGUMENT and a message.
- * The first call on a device looks the array up (cudaGetSymbolAddress); make
- * that first call before any stream capture. Calls share the array: calls
- * that overlap on the GPU (other streams or threads) race; calls on one
- * stream are ordered. Frames and d_oob as for dream_das_batch_create/_run.
+ * The first call on a device looks the array up (cudaGetSymbolAddress). Each
+ * call stages its frame table and tile list in a host array that the next call
+ * rewrites and copies them to the device on the stream, so a stream that is
+ * being captured into a CUDA graph is refused (DREAM_ERR_UNSUPPORTED); use
+ * dream_das_batch_run for captured batches. Calls share the array: calls that
+ * overlap on the GPU (other streams or threads) race; calls on one stream are
+ * ordered. Frames (validated exactly as by dream_das_batch_create) and d_oob
+ * as for dream_das_batch_create/_run.
  */
 int dream_das_batch_run_noalloc(const dream_das_frame *frames, int n_frames, int precision,
                                 int device, unsigned long long *d_oob, void *stream);
