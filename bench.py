@@ -334,12 +334,18 @@ def rca_bench(dev, steps: int = 3):
     f = lambda a, dt: torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=dt).T)).to(dev).t()
     out = {"config": "RCA 128x128 row-tx, K=4096, 128x128x256 grid", "sums": int(Ro.shape[0]) * 128 * 128}
     d_oob = torch.zeros(1, dtype=torch.int64, device=dev)
-    for name, prec in (("f32_store", _lib.PREC_F32_STORE), ("bf16_store", _lib.PREC_BF16_STORE),
-                       ("plain_f32", _lib.PREC_F32)):
+    images = {}
+    for name, prec in (("plain_f64", _lib.PREC_F64), ("f32_store", _lib.PREC_F32_STORE),
+                       ("bf16_store", _lib.PREC_BF16_STORE), ("plain_f32", _lib.PREC_F32)):
         geo = np.float32 if prec == _lib.PREC_F32 else np.float64
         Gt_d, Gr_d, Ro_d, dl = f(Gc, geo), f(Gr_, geo), f(Ro, geo), f(np.zeros((1, 1)), geo)
-        Yd = Y.t().contiguous().to(torch.bfloat16).t() if prec == _lib.PREC_BF16_STORE else Y
-        Im = torch.empty(Ro.shape[0], device=dev, dtype=torch.float32)
+        if prec == _lib.PREC_BF16_STORE:
+            Yd = Y.t().contiguous().to(torch.bfloat16).t()
+        elif prec == _lib.PREC_F64:
+            Yd = Y.t().contiguous().double().t()
+        else:
+            Yd = Y
+        Im = torch.empty(Ro.shape[0], device=dev, dtype=torch.float64 if prec == _lib.PREC_F64 else torch.float32)
         plan = _lib.plan_create(_lib.RCA_ROWTX, 4096, Ro.shape[0], 128, 128, prec, dev.index)
         if prec != _lib.PREC_F32:
             _lib.check(L.dream_das_set_grid_hint(plan.handle, grid_hint(Ro)))
@@ -357,7 +363,15 @@ def rca_bench(dev, steps: int = 3):
         torch.cuda.synchronize()
         ms = a.elapsed_time(e) / steps
         out[name] = {"ms_per_frame": ms, "gsum_s": out["sums"] / ms / 1e6}
+        images[name] = Im.double()
         del Yd
+    ref = images["plain_f64"]
+    scale = float(ref.abs().max())
+    for name in ("f32_store", "bf16_store", "plain_f32"):
+        out[name]["max_rel_err_vs_fp64"] = float((images[name] - ref).abs().max()) / scale
+        out[name]["vs_plain_f64"] = out["plain_f64"]["ms_per_frame"] / out[name]["ms_per_frame"]
+    out["error_note"] = ("max |Im - Im_fp64| / max |Im_fp64| over all 4.19M points; Im_fp64 = the plain FP64 kernel "
+                         "(bit-identical to the reference das) on the same samples")
     return out
 
 
@@ -580,14 +594,84 @@ def batch_bench(dev, steps: int = 10, n_frames: int = 48):
     e.record()
     torch.cuda.synchronize()
     ms = a.elapsed_time(e) / steps
+    oob_per_batch = b.oob_count() // (steps + 3 + 1)  # the counter accumulates over every replay and the capture run
     return {"config": f"{n_frames} uneven TFM frames, FP32 storage, persistent launch in a CUDA graph",
-            "sums_per_batch": b.sums, "ms_per_batch": ms, "gsum_s": b.sums / ms / 1e6, "work_items": b.items,
-            "persistent_ctas": b.grid, "autotune_s": tune_s, "oob_terms": b.oob_count()}
+            "sums_per_batch": b.sums, "in_bounds_sums_per_batch": b.sums - oob_per_batch,
+            "oob_sums_per_batch": oob_per_batch, "ms_per_batch": ms, "gsum_s": b.sums / ms / 1e6,
+            "in_bounds_gsum_s": (b.sums - oob_per_batch) / ms / 1e6, "work_items": b.items,
+            "persistent_ctas": b.grid, "autotune_s": tune_s}
+
+
+def tfm_extras(dev, scene, plain_f64_ms: float, Im_f64, steps: int = 10, n_copies: int = 8):
+    """On the TFM frame itself: the persistent batch kernel over n_copies of
+    the frame (the same A-scans, images to separate buffers), and the
+    geometry-bound operator's adjoint (scatter) and forward; each against the
+    plain FP64 kernel's time on the frame. The batch images are checked
+    against the FP64 image (max relative error)."""
+    import torch
+    from dream_b200.autograd import DASOperator
+    from dream_b200.batch import DASBatch, make_frame
+    f0 = make_frame(scene.Y, scene.Gt, scene.Gr, scene.Ro, scene.dt, scene.delay, scene.cp, "tfm", device=dev)
+    frames = [f0]
+    for _ in range(n_copies - 1):
+        f = make_frame(f0.Y, f0.Gt, f0.Gr, f0.Ro, scene.dt, scene.delay, scene.cp, "tfm", device=dev)
+        frames.append(f)
+    b = DASBatch(frames)
+    g = b.capture()
+    for _ in range(3):
+        g.replay()
+    torch.cuda.synchronize()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    ms = []
+    for i in range(steps):
+        flush.fill_(float(i))
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        g.replay()
+        e.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(e))
+    ms_frame = min(ms) / n_copies
+    scale = float(Im_f64.abs().max())
+    err = max(float((f.Im.double() - Im_f64).abs().max()) for f in frames) / scale
+    out = {"batch_tfm": {"frames": n_copies, "ms_per_frame": ms_frame, "gsum_s": scene.sums / ms_frame / 1e6,
+                         "vs_plain_f64": plain_f64_ms / ms_frame, "max_rel_err_vs_fp64": err,
+                         "note": "persistent batch kernel over copies of the TFM frame in one CUDA graph; L2 flushed "
+                                 "before each replay"}}
+    del g, b
+    op = DASOperator(scene.Gt, scene.Gr, scene.Ro, scene.dt, scene.delay, scene.cp, "tfm", scene.Y.shape[0],
+                     device=dev)
+    gen = torch.Generator(device=dev).manual_seed(3)
+    x = torch.randn(op.No, device=dev, generator=gen)
+    Yd = f0.Y
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        t = []
+        for i in range(steps):
+            flush.fill_(float(i))
+            a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            e.record()
+            torch.cuda.synchronize()
+            t.append(a.elapsed_time(e))
+        return min(t)
+    t_adj = timed(lambda: op.adjoint(x))
+    t_fwd = timed(lambda: op.forward(Yd))
+    out["adjoint_tfm"] = {"ms_per_frame": t_adj, "gsum_s": scene.sums / t_adj / 1e6,
+                          "vs_plain_f64": plain_f64_ms / t_adj,
+                          "note": "geometry-bound operator's adjoint (scatter of an N(0,1) image onto the 3000 x 4096 "
+                                  "A-scans, zeroing included) on the TFM frame; L2 flushed before each call"}
+    out["operator_forward_tfm"] = {"ms_per_frame": t_fwd, "gsum_s": scene.sums / t_fwd / 1e6,
+                                   "vs_plain_f64": plain_f64_ms / t_fwd}
+    return out
 
 
 CASES = ("fast_f32", "fast_bf16", "plain_f64", "plain_f32", "saft_fast", "saft_plain_f64", "uni_f32",
-         "batch", "op_gather", "op_adjoint", "op_wgrad", "op_backward", "rca_bf16", "rca_f32", "conv_dp", "conv_pulse",
-         "sir_field", "sir_arr", "conv_fmc")
+         "batch", "op_gather", "op_adjoint", "op_wgrad", "op_backward", "adjoint_tfm", "rca_bf16", "rca_f32", "conv_dp",
+         "conv_pulse", "sir_field", "sir_arr", "conv_fmc")
 
 
 def run_case(name: str, repeat: int = 3):
@@ -599,6 +683,7 @@ def run_case(name: str, repeat: int = 3):
       uni_f32                                        das_uni TFM 64x64, K=3000, 512x512 (FP32)
       batch                                          the first 12 of the 48 uneven batch frames
       op_gather / op_adjoint / op_wgrad / op_backward  CG configuration 32x32, K=2048, 256x256
+      adjoint_tfm                                    the operator's adjoint on the TFM 64x64, K=3000, 512x512 frame
       rca_bf16 / rca_f32                             RCA 128x128 row-tx, K=4096, 128x128x256 grid
       conv_dp / conv_pulse                           fftconv_p of the TFM synthesis: 2000x101 SIRs with a
                                                      2000-sample column / 3999x101 with the 150-sample pulse
@@ -614,7 +699,7 @@ def run_case(name: str, repeat: int = 3):
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     t = lambda a, dt=np.float64: torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=dt).T)).to(dev).t()
-    if name in ("fast_f32", "fast_bf16", "plain_f64", "plain_f32", "uni_f32"):
+    if name in ("fast_f32", "fast_bf16", "plain_f64", "plain_f32", "uni_f32", "adjoint_tfm"):
         sc = synth.tfm_scene(seed=1)
     elif name.startswith("saft"):
         sc = synth.saft_scene(seed=0)
@@ -658,6 +743,11 @@ def run_case(name: str, repeat: int = 3):
         Y = op.adjoint(x, w)  # A-scans synthesised from the reflectivity (the CG forward model)
         fn = {"op_gather": lambda: op.forward(Y, w), "op_adjoint": lambda: op.adjoint(x, w),
               "op_wgrad": lambda: op.wgrad(x, Y), "op_backward": lambda: op.backward(x, Y, w)}[name]
+    elif name == "adjoint_tfm":
+        from dream_b200.autograd import DASOperator
+        op = DASOperator(sc.Gt, sc.Gr, sc.Ro, sc.dt, sc.delay, sc.cp, "tfm", sc.Y.shape[0], device=dev)
+        x = torch.randn(op.No, device=dev, generator=torch.Generator(device=dev).manual_seed(3))
+        fn = lambda: op.adjoint(x)
     elif name in ("rca_bf16", "rca_f32"):
         Yr, Gc, Grow, Ro = synth.rca_frame_torch(device=dev)
         if name == "rca_bf16":
@@ -810,13 +900,26 @@ def main():
     tot_h, launches_h, Im_h = variant(_lib.PREC_F32_STORE, args.steps, args.warmup)
     clk = clocks.stop()
     side = max(3, args.steps // 4)
-    others = {}
+    others, images = {}, {"f32_store": Im_h.double()}
     for name, code in (("bf16_store", _lib.PREC_BF16_STORE), ("plain_f32", _lib.PREC_F32),
                        ("plain_f64", _lib.PREC_F64)):
-        t, _, _ = variant(code, side, max(3, args.warmup // 2))
+        t, _, Im_v = variant(code, side, max(3, args.warmup // 2))
         others[name] = {"gsum_s": world * sums / (t / side * 1e-3) / 1e9, "ms_per_frame": t / side}
+        images[name] = Im_v.double()
 
     step_ms = tot_h / args.steps
+    # image error of every variant against the plain FP64 image (bit-identical to the reference das),
+    # computed after the timing
+    Im64 = images["plain_f64"]
+    scale64 = float(Im64.abs().max())
+    variants = dict({"f32_store": {"gsum_s": world * sums / (step_ms * 1e-3) / 1e9, "ms_per_frame": step_ms}},
+                    **others)
+    for name in ("f32_store", "bf16_store", "plain_f32"):
+        variants[name]["max_rel_err_vs_fp64"] = float((images[name] - Im64).abs().max()) / scale64
+        variants[name]["vs_plain_f64"] = others["plain_f64"]["ms_per_frame"] / variants[name]["ms_per_frame"]
+    variants["error_note"] = ("max |Im - Im_fp64| / max |Im_fp64| over all 262,144 points; Im_fp64 = the plain FP64 "
+                              "kernel, bit-identical to the reference das (tests/test_gpu_das_parity.py)")
+    extras = tfm_extras(dev, scene, others["plain_f64"]["ms_per_frame"], Im64)
     value = world * sums / (step_ms * 1e-3) / 1e9
 
     # ---- e2e through the public API from pinned host memory ----
@@ -864,10 +967,12 @@ def main():
     if rank != 0:
         return
 
-    peak, peak_kind = measured_peaks()
+    hbm_peak, peak_kind = measured_peaks()
     gathered = sums * 4  # one FP32 sample gathered per sum
     achieved = gathered / (step_ms * 1e-3) / 1e9
     compulsory = s32.Y.nbytes + s32.Ro.nbytes + No * 4 + (Nt + Nr) * 12
+    l2peak = peaks.get("l2_random_sector_GBps")
+    l2l1 = read_traffic("das_fast_f32_tfm", 2)
     line = {
         "metric": METRIC, "value": value, "unit": "Gsum/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
@@ -877,15 +982,29 @@ def main():
                    "precision": "FP32-stored A-scans, FP32 compensated sums, FP64-exact sample indices",
                    "l2": "flushed between timed steps (256 MiB write, outside the timed events)",
                    "parallelism": f"{world} independent frames, one per GPU"},
-        "variants": dict({"f32_store": {"gsum_s": value, "ms_per_frame": step_ms}}, **others),
+        "variants": variants,
+        "batch_tfm": extras["batch_tfm"],
+        "adjoint_tfm": extras["adjoint_tfm"],
+        "operator_forward_tfm": extras["operator_forward_tfm"],
         "e2e": {"value": e2e_val, "unit": "Gsum/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "api": "dream_b200.beamformer.das_mixed(pinned host arrays, device='cuda', storage='f32')"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+        "roofline": {"bound": "l2", "achieved": achieved, "peak": l2peak, "unit": "GB/s",
+                     "frac": achieved / l2peak if l2peak else None,
                      "traffic": read_traffic("das_fast_f32_tfm"),
-                     "peak_source": f"{peak_kind} hbm_gbs",
+                     "traffic_source": "profiles/ncu_traffic.txt: dram__bytes_read.sum + dram__bytes_write.sum of "
+                                       "one ncu capture of `python bench.py --case fast_f32`",
                      "algorithmic_bytes_per_launch": gathered,
-                     "note": "achieved = gathered sample bytes (4 B per sum) / kernel time",
-                     "compulsory_hbm_frac": compulsory / (step_ms * 1e-3) / 1e9 / peak},
+                     "peak_source": "L2 random 32-byte-sector read rate measured in this run (dream_b200/peaks)",
+                     "l2_to_l1_bytes_per_launch": l2l1,
+                     "l2_sector_frac": (l2l1 / (step_ms * 1e-3) / 1e9 / l2peak) if (l2l1 and l2peak) else None,
+                     "hbm_compulsory_frac": compulsory / (step_ms * 1e-3) / 1e9 / hbm_peak,
+                     "hbm_peak": hbm_peak, "hbm_peak_source": f"{peak_kind} hbm_gbs",
+                     "note": "achieved = gathered sample bytes (4 B per sum) / kernel time, against the rate at "
+                             "which L2 serves random sectors; the gathers are served by L1 and L2 (the 49 MB of "
+                             "A-scans are L2-resident), so the DRAM traffic is the compulsory bytes only "
+                             "(hbm_compulsory_frac). l2_sector_frac = L2->L1 sector bytes per launch (ncu) over "
+                             "the kernel time, against the same rate. The kernel is limited by instruction "
+                             "issue and gather latency (profiles/das_fast_f32_tfm_64x64_K3000_512x512.md)."},
         "adjoint_cg": cg,
         "batched": batched,
         "rca": rca,

@@ -57,6 +57,7 @@ SIGNATURES = {
     "dream_das_set_grid_hint": (_i, [_vp, _i64]),
     "dream_das_set_tile": (_i, [_vp, _i, _i]),
     "dream_das_set_chunk": (_i, [_vp, _i]),
+    "dream_das_set_inner_shard": (_i, [_vp, _i64, _i64]),
     "dream_das_set_l2_block": (_i, [_vp, _i64]),
     "dream_das_indices_device": (_i, [_vp, _vp, _vp, _vp, _d, _i, _vp, _d, _vp, _vp, _vp]),
     "dream_conv_p_run_device": (_i, [_vp, _i64, _i64, _vp, _i64, _i64, _vp, _i, _vp]),

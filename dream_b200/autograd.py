@@ -34,7 +34,7 @@ class DASOperator:
     the bound plan); K is the A-scan length.
     """
 
-    def __init__(self, Gt, Gr, Ro, dt, delay, cp, method, K, device="cuda"):
+    def __init__(self, Gt, Gr, Ro, dt, delay, cp, method, K, device="cuda", inner=None):
         self.device = torch.device(device) if not isinstance(device, torch.device) else device
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
@@ -49,6 +49,16 @@ class DASOperator:
         self.No = int(self.Ro.shape[0])
         self.Nt, self.Nr = int(self.Gt.shape[0]), int(self.Gr.shape[0])
         self.ncol = self.Nt * self.Nr
+        self.inner = None
+        if inner is not None:
+            # an inner-element shard: the A-scans are the columns of inner elements [lo, hi)
+            from .beamformer import inner_count
+            lo, hi = int(inner[0]), int(inner[1])
+            n_out, n_in = inner_count(das_type, self.Nt, self.Nr)
+            if not (0 <= lo < hi <= n_in):
+                raise RuntimeError("DASOperator: inner-element shard out of range")
+            self.inner = (lo, hi)
+            self.ncol = n_out * (hi - lo)
         multi = self.delay.numel() > 1
         if multi and self.delay.numel() != self.No:
             raise RuntimeError("Error in das!")
@@ -57,6 +67,8 @@ class DASOperator:
         L = _lib.load()
         h = grid_hint(self.Ro)
         _lib.check(L.dream_das_set_grid_hint(self.plan.handle, h))
+        if self.inner is not None:
+            _lib.check(L.dream_das_set_inner_shard(self.plan.handle, *self.inner))
         self._L = L
         _lib.check(L.dream_das_bind_geometry(
             self.plan.handle, _p(self.Ro), _p(self.Gt), _p(self.Gr), float(dt),

@@ -101,9 +101,10 @@ def _rows_cols(a):
     raise RuntimeError("arguments must be vectors or matrices")
 
 
-def _check_shapes(Y, Gt, Gr, Ro, delay, das_type):
+def _check_shapes(Y, Gt, Gr, Ro, delay, das_type, count_columns=True):
     """Shape checks of python/include/py_das.hpp:53-124, plus the A-scan count
-    (the reference reads past Y when it has too few columns; here it is an error)."""
+    (the reference reads past Y when it has too few columns; here it is an error;
+    count_columns=False leaves the count to the caller)."""
     K, C = _rows_cols(Y)
     if _rows_cols(Gt)[1] != 3:
         raise RuntimeError("Argument 2 must be a (num transmit elements) x 3 matrix!")
@@ -122,7 +123,7 @@ def _check_shapes(Y, Gt, Gr, Ro, delay, das_type):
         raise RuntimeError("Error in das!")
     eff = _lib.SAFT if (das_type == _lib.SAFT or Nr == 0) else das_type
     need = Nt if eff == _lib.SAFT else Nt * Nr
-    if C < need:
+    if count_columns and C < need:
         raise RuntimeError(f"das: Y has {C} A-scans but the method needs {need}")
     return K, No, Nt, Nr, (dlen > 1)
 
@@ -144,6 +145,7 @@ def das_generic(dtype, Y, Gt, Gr, Ro, dt, delay, cp, method, err_level="stop", d
     prec = _lib.PREC_F64 if np.dtype(dtype) == np.float64 else _lib.PREC_F32
     key = ("das", das_type, K, No, Nt, Nr, prec, dev)
     plan = _plan(key, lambda: _lib.plan_create(das_type, K, No, Nt, Nr, prec, dev))
+    _set_hint(plan, grid_hint(Ro))
     Im = np.zeros(No, dtype=dtype)
     oob = ctypes.c_int64(0)
     p = lambda a: a.ctypes.data_as(ctypes.c_void_p) if a is not None and a.size else None
@@ -153,6 +155,14 @@ def das_generic(dtype, Y, Gt, Gr, Ro, dt, delay, cp, method, err_level="stop", d
         p(Im), level, ctypes.byref(oob)))
     _report(st)
     return Im
+
+
+def _set_hint(plan, h):
+    """The plan's grid hint (only speed depends on it: the plain kernels give
+    each warp an 8 x 4 patch of the grid instead of 32 consecutive points)."""
+    if getattr(plan, "hint", None) != h:
+        _lib.check(_lib.load().dream_das_set_grid_hint(plan.handle, int(h)))
+        plan.hint = h
 
 
 def _torch_fortran(t, dtype, device):
@@ -186,6 +196,7 @@ def _das_torch(dtype, Y, Gt, Gr, Ro, dt, delay, cp, das_type, level, dev):
     prec = _lib.PREC_F64 if np.dtype(dtype) == np.float64 else _lib.PREC_F32
     key = ("das", das_type, K, No, Nt, Nr, prec, dev)
     plan = _plan(key, lambda: _lib.plan_create(das_type, K, No, Nt, Nr, prec, dev))
+    _set_hint(plan, grid_hint(Ro))
     Im = torch.empty(No, dtype=Y.dtype, device=device)
     oob = ctypes.c_int64(0)
     stream = torch.cuda.current_stream(device).cuda_stream
@@ -337,14 +348,23 @@ def _das_mixed_host(Y, Gt, Gr, Ro, dt, delay, cp, das_type, level, dev, prec, hi
     return out
 
 
+def inner_count(das_type: int, Nt: int, Nr: int) -> tuple:
+    """(outer, inner) element counts of a TFM / RCA frame: RCA row-tx loops
+    over rows (Gr) outside and columns (Gt) inside, the others Gt outside."""
+    return (Nr, Nt) if das_type == _lib.RCA_ROWTX else (Nt, Nr)
+
+
 def das_mixed(Y, Gt, Gr, Ro, dt, delay, cp, method, err_level="stop", device="cuda", storage="f32",
-              weights=None, hint="auto", tile=None, stream=None):
+              weights=None, hint="auto", tile=None, stream=None, inner=None):
     """DAS with A-scans stored in FP32 (``storage='f32'``) or BF16 and FP32
     compensated accumulation; sample indices are the FP64 reference's.
 
     Geometry and delays are taken in FP64. Returns an FP32 image (a torch
     tensor on the device when Y is a CUDA tensor, else a NumPy array).
     ``weights`` (one per A-scan column) gives ``sum_c w[c] * Y[k, c]``.
+    ``inner=(lo, hi)``: Y holds only the A-scans of inner elements [lo, hi)
+    (column o * (hi - lo) + i - lo; see ``inner_count``) and the result is the
+    partial image over those terms (dream_das_set_inner_shard).
     """
     import torch
     das_type = parse_method(method)
@@ -352,7 +372,7 @@ def das_mixed(Y, Gt, Gr, Ro, dt, delay, cp, method, err_level="stop", device="cu
     dev = parse_device(device)
     prec = _STORAGE[storage]
     on_host = not (_is_torch(Y) and Y.device.type == "cuda")
-    if on_host and weights is None and stream is None:
+    if on_host and weights is None and stream is None and inner is None:
         return _das_mixed_host(Y, Gt, Gr, Ro, dt, delay, cp, das_type, level, dev, prec, hint, tile)
     device_t = Y.device if not on_host else torch.device("cuda", dev)
     dev = device_t.index if device_t.index is not None else torch.cuda.current_device()
@@ -364,7 +384,19 @@ def das_mixed(Y, Gt, Gr, Ro, dt, delay, cp, method, err_level="stop", device="cu
     Gr_t = _torch_fortran(Gr, np.float64, device_t) if Gr is not None and das_type != _lib.SAFT else None
     Ro_t = _torch_fortran(Ro, np.float64, device_t)
     dl_t = _torch_fortran(delay, np.float64, device_t)
-    K, No, Nt, Nr, multi = _check_shapes(Yt, Gt_t, Gr_t, Ro_t, dl_t, das_type)
+    if inner is not None and weights is not None:
+        raise RuntimeError("das: weights and an inner-element shard cannot be combined")
+    if inner is None:
+        K, No, Nt, Nr, multi = _check_shapes(Yt, Gt_t, Gr_t, Ro_t, dl_t, das_type)
+    else:
+        lo, hi = int(inner[0]), int(inner[1])
+        K, C = _rows_cols(Yt)
+        _, No, Nt, Nr, multi = _check_shapes(Yt, Gt_t, Gr_t, Ro_t, dl_t, das_type, count_columns=False)
+        n_out, n_in = inner_count(das_type, Nt, Nr)
+        if das_type == _lib.SAFT or not (0 <= lo < hi <= n_in):
+            raise RuntimeError("das: inner-element shard out of range")
+        if C != n_out * (hi - lo):
+            raise RuntimeError(f"das: an inner-element shard [{lo}, {hi}) needs {n_out * (hi - lo)} A-scans, got {C}")
     h = grid_hint(Ro if not on_host else np.asarray(Ro)) if hint == "auto" else int(hint or 0)
     plan = _fast_plan(das_type, K, No, Nt, Nr, prec, dev, h, tile)
     Im = torch.empty(No, dtype=torch.float32, device=device_t)
@@ -381,6 +413,12 @@ def das_mixed(Y, Gt, Gr, Ro, dt, delay, cp, method, err_level="stop", device="cu
             raise RuntimeError(f"das: weights need {need} values (one per A-scan column)")
         _lib.check(L.dream_das_weighted_run_device(*common, ptr(w), ptr(Im), ptr(d_oob),
                                                    ctypes.c_void_p(st_)))
+    elif inner is not None:
+        _lib.check(L.dream_das_set_inner_shard(plan.handle, lo, hi))
+        try:
+            _lib.check(L.dream_das_run_device_async(*common, ptr(Im), ptr(d_oob), ctypes.c_void_p(st_)))
+        finally:
+            _lib.check(L.dream_das_set_inner_shard(plan.handle, 0, 0))
     else:
         _lib.check(L.dream_das_run_device_async(*common, ptr(Im), ptr(d_oob), ctypes.c_void_p(st_)))
     oob = int(d_oob.item())

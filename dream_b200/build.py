@@ -29,7 +29,8 @@ PEAKS_LIB = os.path.join(HERE, "libdream_peaks.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fno-fast-math",
-           "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
+           "-Xcompiler", "-ffp-contract=off", "-Xcompiler", "-Werror=infinite-recursion",
+           "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
 
 
 def nvcc() -> str:

@@ -130,13 +130,15 @@ struct dream_das_plan {
   int tile_f = 0, tile_s = 0;  // user / autotuner tile (0: automatic)
   int jc = 0;                  // user / autotuner inner chunk (0: automatic)
   int64_t l2_block = 0;        // A-scan bytes per inner-element pass (0: automatic, < 0: never split)
+  // inner-element shard: Y holds only inner elements [shard_lo, shard_hi) (0, 0: all of them)
+  int64_t shard_lo = 0, shard_hi = 0;
   // host-pointer runs of FP32/BF16-storage plans: A-scan upload stream
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t chunk_ev[16] = {nullptr};  // [0, 15): upload chunks, [15]: fence on the previous call
   // geometry-bound operator
   bool bound = false;
   FastParams geo{};
-  DevBuf bTA, bTB, bRange;
+  DevBuf bScatter;  // unweighted scatter of the weight gradient (bound operator)
   DevBuf bBad;  // gather index violations (bounds-checked builds only)
   int sm_count = 148;
   unsigned long long *h_oob = nullptr;  // pinned
@@ -248,14 +250,27 @@ unsigned long long *bad_counter(dream_das_plan *p) {
 int launch_plain(dream_das_plan *p, PlainLaunch &L, cudaStream_t st) {
   L.ny = p->K * num_columns(p);
   L.bad = bad_counter(p);
+  // 2-D warp patches when the plan has a grid hint (das_uni: its own grid)
+  L.n_fast = 0;
+  if (L.uni) {
+    const int64_t nf = L.Ny > 1 ? L.Ny : L.Ny * L.Nz;
+    if (nf >= 8 && L.No % nf == 0 && nf < L.No) L.n_fast = nf;
+  } else if (p->n_fast >= 8 && p->n_fast < L.No) {
+    L.n_fast = p->n_fast;
+  }
   // Pixel chunks keep a cancellation request observable between launches.
   const int64_t tpp = std::max<int64_t>(terms_per_pixel(p), 1);
   int64_t chunk = std::max<int64_t>(int64_t(1) << 16, (int64_t(1) << 33) / tpp);
   chunk = (chunk + 255) / 256 * 256;
-  for (int64_t s = 0; s < L.No; s += chunk) {
+  int64_t total = L.No;
+  if (L.n_fast > 0) {  // the range is over 8 x 4 warp patches
+    total = ((L.n_fast + 7) / 8) * ((L.No / L.n_fast + 3) / 4);
+    chunk = std::max<int64_t>(8, chunk / 32);
+  }
+  for (int64_t s = 0; s < total; s += chunk) {
     if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
     L.no0 = s;
-    L.no1 = std::min(L.No, s + chunk);
+    L.no1 = std::min(total, s + chunk);
     cudaError_t e = (p->precision == DREAM_PREC_F64) ? launch_plain_f64(L, st) : launch_plain_f32(L, st);
     if (e != cudaSuccess) return cuda_fail(e, "DAS kernel launch");
     p->launches++;
@@ -338,6 +353,56 @@ void fast_tile(const dream_das_plan *p, int n_out, int &tf, int &ts, int &wf) {
   }
 }
 
+// Tiling of the FP32/BF16-storage kernels for plan p: tile shape, warp
+// layout, register chunk and grid axes (F.method, Nt, Nr, No must be set).
+int tile_params(const dream_das_plan *p, FastParams &F, int jc) {
+  const int n_out = (F.method == DREAM_DAS_RCA_ROWTX) ? F.Nr : F.Nt;
+  fast_tile(p, n_out, F.tile_f, F.tile_s, F.wf);
+  F.jc = jc ? jc : (p->jc ? p->jc : 16);
+  if (p->n_fast > 0) {
+    F.n_fast = p->n_fast;
+    F.n_slow = p->No / p->n_fast;
+  } else {
+    F.n_fast = p->No;
+    F.n_slow = 1;
+  }
+  if (fast_smem_bytes(F, F.tile_f * F.tile_s) > 220 * 1024)
+    return fail(DREAM_ERR_UNSUPPORTED, "too many elements on the outer loop for the FP32/BF16 storage kernels");
+  return 0;
+}
+
+// The plan's inner-element shard (dream_das_set_inner_shard) applied to F:
+// column layout of the shard's A-scans and the inner range; false when the
+// range leaves nothing to do.
+bool apply_shard(const dream_das_plan *p, FastParams &F) {
+  if (p->shard_hi <= 0) return true;
+  const int n_out = (F.method == DREAM_DAS_RCA_ROWTX) ? F.Nr : F.Nt;
+  const int n_in = (F.method == DREAM_DAS_RCA_ROWTX) ? F.Nt : F.Nr;
+  F.ycol_o = p->shard_hi - p->shard_lo;
+  F.ycol_i0 = (int)p->shard_lo;
+  F.ny = p->K * n_out * F.ycol_o;
+  const int lo = std::max<int>(F.in_lo, (int)p->shard_lo);
+  const int hi = std::min<int>(F.in_hi > 0 ? F.in_hi : n_in, (int)p->shard_hi);
+  F.in_lo = lo;
+  F.in_hi = hi;
+  return lo < hi;
+}
+
+// A-scan columns the plan's Y holds: all of them, or the shard's.
+int64_t plan_columns(const dream_das_plan *p) {
+  if (p->shard_hi <= 0) return num_columns(p);
+  const int64_t n_out = (effective_method(p) == DREAM_DAS_RCA_ROWTX) ? p->Nr : p->Nt;
+  return n_out * (p->shard_hi - p->shard_lo);
+}
+
+// Slow-axis tiles per launch: about 2^34 terms, so a launch stays well below
+// a second.
+int64_t slow_tile_chunk(const FastParams &F, int64_t terms_per_pixel) {
+  const int64_t per_tile_terms = (int64_t)F.tile_s * F.n_fast * terms_per_pixel;
+  const int64_t chunk = std::max<int64_t>(1, (int64_t(1) << 34) / std::max<int64_t>(per_tile_terms, 1));
+  return std::min<int64_t>(chunk, 65535);
+}
+
 int launch_fast_plan(dream_das_plan *p, const void *dY, const void *dRo, const void *dGt, const void *dGr,
                      double dt, int delay_type, const void *ddelay, double cp, const float *dW, float *dIm,
                      unsigned long long *doob, cudaStream_t st, int in_lo = 0, int in_hi = 0, int accumulate = 0,
@@ -394,26 +459,16 @@ int launch_fast_plan(dream_das_plan *p, const void *dY, const void *dRo, const v
     return 0;
   }
   const int n_out = (method == DREAM_DAS_RCA_ROWTX) ? F.Nr : F.Nt;
-  fast_tile(p, n_out, F.tile_f, F.tile_s, F.wf);
-  F.jc = jc ? jc : (p->jc ? p->jc : 16);
-  if (p->n_fast > 0) {
-    F.n_fast = p->n_fast;
-    F.n_slow = p->No / p->n_fast;
-  } else {
-    F.n_fast = p->No;
-    F.n_slow = 1;
-  }
-  if (fast_smem_bytes(F, F.tile_f * F.tile_s) > 220 * 1024)
-    return fail(DREAM_ERR_UNSUPPORTED, "too many elements on the outer loop for the FP32/BF16 storage kernels");
+  int r = tile_params(p, F, jc);
+  if (r) return r;
   const int64_t slow_tiles = (F.n_slow + F.tile_s - 1) / F.tile_s;
-  const int64_t per_tile_terms = (int64_t)F.tile_s * F.n_fast * tpp;
-  int64_t chunk = std::max<int64_t>(1, (int64_t(1) << 34) / std::max<int64_t>(per_tile_terms, 1));
-  chunk = std::min<int64_t>(chunk, 65535);
+  const int64_t chunk = slow_tile_chunk(F, tpp);
   // L2 blocking: A-scans larger than the budget are beamformed in passes over
   // ranges of inner elements (multiples of the 16-term register chunk), each
   // pass adding its terms into the image, so the A-scans of one pass stay in
   // L2 while every image point gathers from them.
   const int n_in = (method == DREAM_DAS_RCA_ROWTX) ? F.Nt : F.Nr;
+  if (!apply_shard(p, F)) return 0;  // Y holds the columns of inner elements [shard_lo, shard_hi) only
   const int64_t col_bytes = (int64_t)n_out * p->K * (bf16 ? 2 : 4);  // A-scans of one inner element
   const int64_t y_bytes = col_bytes * n_in;
   // automatic: passes of at most 96 MB once the A-scans exceed 160 MB (RCA
@@ -515,9 +570,7 @@ void dream_das_plan_destroy(dream_das_plan *p) {
     p->bIm.release();
     p->bOob.release();
     p->bY16.release();
-    p->bTA.release();
-    p->bTB.release();
-    p->bRange.release();
+    p->bScatter.release();
     if (p->h_oob) cudaFreeHost(p->h_oob);
     for (auto &ev : p->chunk_ev)
       if (ev) cudaEventDestroy(ev);
@@ -597,6 +650,25 @@ int dream_das_set_l2_block(dream_das_plan *p, int64_t bytes) {
   DREAM_API_CATCH
 }
 
+int dream_das_set_inner_shard(dream_das_plan *p, int64_t lo, int64_t hi) {
+  DREAM_API_TRY
+  if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
+  if (!is_fast(p) || p->uni)
+    return fail(DREAM_ERR_UNSUPPORTED, "inner-element shards need an F32_STORE or BF16_STORE das plan");
+  const int method = effective_method(p);
+  if (method == DREAM_DAS_SAFT) return fail(DREAM_ERR_UNSUPPORTED, "SAFT has no inner elements to shard");
+  const int64_t n_in = (method == DREAM_DAS_RCA_ROWTX) ? p->Nt : p->Nr;
+  if (lo == 0 && hi == 0) {
+    p->shard_lo = p->shard_hi = 0;
+    return 0;
+  }
+  if (lo < 0 || hi > n_in || lo >= hi) return fail(DREAM_ERR_ARGUMENT, "inner-element shard out of range");
+  p->shard_lo = lo;
+  p->shard_hi = hi;
+  return 0;
+  DREAM_API_CATCH
+}
+
 int dream_das_set_chunk(dream_das_plan *p, int jc) {
   DREAM_API_TRY
   if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
@@ -634,8 +706,7 @@ int dream_das_bind_geometry(dream_das_plan *p, const void *dRo, const void *dGt,
   if ((p->No > 0 && dRo == nullptr) || dGt == nullptr || dGr == nullptr || ddelay == nullptr)
     return fail(DREAM_ERR_ARGUMENT, "NULL device pointer");
   std::lock_guard<std::mutex> lk(p->mu);
-  DeviceGuard g(p->device);
-  cudaStream_t st = (cudaStream_t)stream;
+  (void)stream;  // nothing is precomputed: the operator's kernels form their legs per tile
   FastParams F;
   memset(&F, 0, sizeof(F));
   F.method = method;
@@ -651,18 +722,56 @@ int dream_das_bind_geometry(dream_das_plan *p, const void *dRo, const void *dGt,
   Consts64 c = constants_f64(dt, cp, 0.0);
   F.Fs = c.Fs;
   F.ocp = c.ocp;
-  int r;
-  const int n_out = (method == DREAM_DAS_RCA_ROWTX) ? F.Nr : F.Nt;
-  const int n_in = (method == DREAM_DAS_RCA_ROWTX) ? F.Nt : F.Nr;
-  if ((r = p->bTA.ensure((size_t)n_out * p->No * 8))) return r;
-  if ((r = p->bTB.ensure((size_t)n_in * p->No * 8))) return r;
-  if ((r = p->bRange.ensure(8 * sizeof(int)))) return r;
-  CU(build_leg_tables(F, (int64_t *)p->bTA.p, (int64_t *)p->bTB.p, (int *)p->bRange.p, st));
-  p->launches += 2;
   p->geo = F;
   p->bound = true;
   return 0;
   DREAM_API_CATCH
+}
+
+// Forward (weighted gather) of the bound operator on pixel tiles.
+static int op_gather(dream_das_plan *p, const float *dY, const float *dW, float *dIm, unsigned long long *d_oob,
+                     cudaStream_t st) {
+  FastParams F = p->geo;
+  F.Y = dY;
+  F.w = dW;
+  F.Im = dIm;
+  F.oob = d_oob;
+  F.ny = p->K * num_columns(p);
+  F.bad = bad_counter(p);
+  int r = tile_params(p, F, 0);
+  if (r) return r;
+  if (!apply_shard(p, F)) return 0;
+  const int64_t slow_tiles = (F.n_slow + F.tile_s - 1) / F.tile_s;
+  const int64_t chunk = slow_tile_chunk(F, terms_per_pixel(p));
+  for (int64_t t0 = 0; t0 < slow_tiles; t0 += chunk) {
+    F.slow_tile0 = t0;
+    F.slow_tile1 = std::min(slow_tiles, t0 + chunk);
+    CU(launch_fast(F, false, st));
+    p->launches++;
+  }
+  return 0;
+}
+
+// Adjoint (scatter) of the bound operator on pixel tiles: Ya zeroed, then
+// every term added at the forward's index.
+static int op_scatter(dream_das_plan *p, const float *X, const float *dW, float *Ya, cudaStream_t st) {
+  const size_t ycount = (size_t)p->K * plan_columns(p);
+  if (ycount) CU(cudaMemsetAsync(Ya, 0, ycount * 4, st));
+  if (p->No == 0 || p->K == 0) return 0;
+  FastParams F = p->geo;
+  F.w = dW;
+  int r = tile_params(p, F, 0);
+  if (r) return r;
+  if (!apply_shard(p, F)) return 0;
+  const int64_t slow_tiles = (F.n_slow + F.tile_s - 1) / F.tile_s;
+  const int64_t chunk = slow_tile_chunk(F, terms_per_pixel(p));
+  for (int64_t t0 = 0; t0 < slow_tiles; t0 += chunk) {
+    F.slow_tile0 = t0;
+    F.slow_tile1 = std::min(slow_tiles, t0 + chunk);
+    CU(launch_scatter(F, X, Ya, st));
+    p->launches++;
+  }
+  return 0;
 }
 
 static int op_check(dream_das_plan *p) {
@@ -681,33 +790,8 @@ int dream_das_op_forward(dream_das_plan *p, const float *dY, const float *dW, fl
   DeviceGuard g(p->device);
   if (p->No == 0) return 0;
   if (p->K == 0) return zero_length_ascans(p, dIm, d_oob, (cudaStream_t)stream);
-  FastParams F = p->geo;
-  F.Y = dY;
-  F.w = dW;
-  F.Im = dIm;
-  F.oob = d_oob;
-  CU(launch_tab_gather(F, (const int64_t *)p->bTA.p, (const int64_t *)p->bTB.p, (const int *)p->bRange.p,
-                       (cudaStream_t)stream));
-  p->launches++;
-  return 0;
+  return op_gather(p, dY, dW, dIm, d_oob, (cudaStream_t)stream);
   DREAM_API_CATCH
-}
-
-static int op_colowner(dream_das_plan *p, const float *X, const float *G, const float *dY, const float *dW, float *Ya,
-                       float *dWg, bool adj, bool wg, cudaStream_t st) {
-  const size_t ycount = (size_t)p->K * num_columns(p);
-  if (adj && ycount) CU(cudaMemsetAsync(Ya, 0, ycount * 4, st));
-  if (wg) CU(cudaMemsetAsync(dWg, 0, (size_t)num_columns(p) * 4, st));
-  if (p->No == 0 || p->K == 0) return 0;
-  FastParams F = p->geo;
-  F.Y = dY;
-  F.w = dW;
-  cudaError_t e = launch_tab_colowner(F, (const int64_t *)p->bTA.p, (const int64_t *)p->bTB.p, X, G, Ya, dWg, adj,
-                                      wg, p->sm_count, st);
-  if (e == cudaErrorInvalidValue) return fail(DREAM_ERR_UNSUPPORTED, "A-scans too long for the adjoint histogram");
-  if (e != cudaSuccess) return cuda_fail(e, "adjoint kernel launch");
-  p->launches++;
-  return 0;
 }
 
 int dream_das_op_adjoint(dream_das_plan *p, const float *dX, const float *dW, float *dYa, void *stream) {
@@ -717,7 +801,7 @@ int dream_das_op_adjoint(dream_das_plan *p, const float *dX, const float *dW, fl
   if (dX == nullptr || dYa == nullptr) return fail(DREAM_ERR_ARGUMENT, "NULL device pointer");
   std::lock_guard<std::mutex> lk(p->mu);
   DeviceGuard g(p->device);
-  return op_colowner(p, dX, nullptr, nullptr, dW, dYa, nullptr, true, false, (cudaStream_t)stream);
+  return op_scatter(p, dX, dW, dYa, (cudaStream_t)stream);
   DREAM_API_CATCH
 }
 
@@ -728,7 +812,15 @@ int dream_das_op_wgrad(dream_das_plan *p, const float *dG, const float *dY, floa
   if (dG == nullptr || dY == nullptr || dWgrad == nullptr) return fail(DREAM_ERR_ARGUMENT, "NULL device pointer");
   std::lock_guard<std::mutex> lk(p->mu);
   DeviceGuard g(p->device);
-  return op_colowner(p, nullptr, dG, dY, nullptr, nullptr, dWgrad, false, true, (cudaStream_t)stream);
+  // dW[c] = sum_n g[n] Y[k(n,c), c] = sum_k Y[k,c] (DAS^T g)[k,c]: the
+  // unweighted scatter of g into the plan's scratch, then one column pass
+  const size_t ycount = (size_t)p->K * plan_columns(p);
+  if ((r = p->bScatter.ensure(std::max<size_t>(ycount, 1) * 4))) return r;
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((r = op_scatter(p, dG, nullptr, (float *)p->bScatter.p, st))) return r;
+  CU(launch_column_dot_scale(dY, (float *)p->bScatter.p, nullptr, dWgrad, p->K, plan_columns(p), st));
+  p->launches++;
+  return 0;
   DREAM_API_CATCH
 }
 
@@ -741,7 +833,13 @@ int dream_das_op_backward(dream_das_plan *p, const float *dG, const float *dY, c
     return fail(DREAM_ERR_ARGUMENT, "NULL device pointer");
   std::lock_guard<std::mutex> lk(p->mu);
   DeviceGuard g(p->device);
-  return op_colowner(p, dG, dG, dY, dW, dYgrad, dWgrad, true, true, (cudaStream_t)stream);
+  // one unweighted scatter S = DAS^T g into dYgrad, then per column
+  // dW[c] = <Y[:,c], S[:,c]> and dYgrad[:,c] = w[c] S[:,c]
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((r = op_scatter(p, dG, nullptr, dYgrad, st))) return r;
+  CU(launch_column_dot_scale(dY, dYgrad, dW, dWgrad, p->K, plan_columns(p), st));
+  p->launches++;
+  return 0;
   DREAM_API_CATCH
 }
 
@@ -1086,6 +1184,8 @@ int dream_das_run(dream_das_plan *p, const void *Y, const void *Ro, const void *
   DREAM_API_TRY
   if (p == nullptr) return fail(DREAM_ERR_ARGUMENT, "plan is NULL");
   if (p->uni) return fail(DREAM_ERR_ARGUMENT, "uniform-grid plan passed to dream_das_run");
+  if (p->shard_hi > 0)
+    return fail(DREAM_ERR_UNSUPPORTED, "inner-element shards run through the device entry points");
   if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
   if (delay == nullptr) return fail(DREAM_ERR_ARGUMENT, "delay pointer is NULL");
   std::lock_guard<std::mutex> lk(p->mu);

@@ -34,6 +34,8 @@
 // 32 gathers of one warp fall on one or two 128-byte lines of the A-scan.
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 #include "das_common.cuh"
 #include "das_fast.h"
 
@@ -105,7 +107,6 @@ struct Pixel {
   double xo, yo, zo, delay_ms, gy_c, gx_r;
 };
 
-__device__ __forceinline__ double A_mul_Fs(const FastParams &P, double leg) { return Ar<double>::mul(leg, P.Fs); }
 
 // Elements in Y: K times the A-scan columns (Nt for SAFT, Nt*Nr otherwise).
 __device__ __forceinline__ int64_t y_count(const FastParams &P) {
@@ -172,23 +173,113 @@ __device__ __noinline__ bool exact_index(const FastParams &P, const Pixel &px, i
   return false;
 }
 
-// Scaled leg -> integer floor and fixed point v = floor << fb + frac (modulo
-// 2^32), the same arithmetic wherever a leg is converted. ok = false for legs
-// of 2^26 samples or more: beyond that the FP64 rounding of A + B is no
-// longer far enough below delta, and the tile takes the exact path.
-__device__ __forceinline__ uint32_t fix_leg(double L, int fb, int &fl, bool &ok) {
-  ok = fabs(L) < 67108864.0;  // 2^26
-  double f = floor(ok ? L : 0.0);
-  fl = (int)f;
-  uint32_t frac = (uint32_t)__double2uint_rn((L - f) * (double)(1u << fb));  // in [0, 2^fb]
-  return ((uint32_t)fl << fb) + frac;
+// Bytes of the tile's shared arrays (TileShared): the host's fast_smem_bytes.
+__host__ __device__ __forceinline__ size_t fast_smem_bytes_dev(const FastParams &P, int n_out, int n_in, int nthr) {
+  (void)P;
+  return 64 * sizeof(double) + 64 * sizeof(int) + (size_t)(2 * (n_out + n_in) + n_out) * sizeof(int) +
+         (size_t)(n_out + 16) * nthr * sizeof(uint32_t);
+}
+
+// A-scan column of term (outer o, inner i): o * n_in + i for a full Y. A Y
+// holding only the columns of inner elements [ycol_i0, ycol_i0 + ycol_o) (an
+// inner-element shard) has ycol_o columns per outer element.
+__device__ __forceinline__ int64_t ycol_outer(const FastParams &P, int n_in, int o) {
+  return (int64_t)o * (P.ycol_o > 0 ? P.ycol_o : n_in);
+}
+__device__ __forceinline__ int64_t ycol_inner(const FastParams &P, int i) { return (int64_t)i - P.ycol_i0; }
+__device__ __forceinline__ int64_t ycol(const FastParams &P, int n_in, int o, int i) {
+  return ycol_outer(P, n_in, o) + ycol_inner(P, i);
+}
+
+// Coordinate differences between image point px and element e (outer or
+// inner), as the reference forms them for each method: TFM uses the element's
+// position; an RCA column (Gt) its x and z with the clamped y offset of the
+// column stripe, an RCA row (Gr) its y and z with the clamped x offset.
+__device__ __forceinline__ void leg_diffs(const FastParams &P, const Pixel &px, bool outer, int e, double &dx,
+                                          double &dy, double &dz) {
+  if (P.method == TFM) {
+    const double *G = outer ? P.Gt : P.Gr;
+    const int N = outer ? P.Nt : P.Nr;
+    dx = __ldg(G + e) - px.xo;
+    dy = __ldg(G + e + N) - px.yo;
+    dz = __ldg(G + e + 2 * N) - px.zo;
+  } else if ((P.method == RCA_COLTX) == outer) {  // a column
+    dx = __ldg(P.Gt + e) - px.xo;
+    dy = px.gy_c;
+    dz = __ldg(P.Gt + e + 2 * P.Nt) - px.zo;
+  } else {  // a row
+    dx = px.gx_r;
+    dy = __ldg(P.Gr + e + P.Nr) - px.yo;
+    dz = __ldg(P.Gr + e + 2 * P.Nr) - px.zo;
+  }
+}
+
+// Fixed-point leg: round(L * 2^fb) modulo 2^32, L = |d| * ocp * Fs + delay * Fs
+// the leg in samples, from cfix = ocp * Fs * 2^fb and dfix = delay * Fs * 2^fb.
+// This is not the reference's rounding chain: it only has to lie within
+// 2^-(fb+1) + 2^-24 of the exact FP64 leg, which holds for |L| and
+// |delay * Fs| below 2^23 (a few units of 2^-53 relative, plus the final
+// rounding); the tile bound keeps every fast-path leg in that range. Adding
+// 1.5 * 2^52 leaves the nearest integer in the low mantissa word.
+__device__ __forceinline__ uint32_t leg_fix(double dx, double dy, double dz, double cfix, double dfix) {
+  const double ss = fma(dz, dz, fma(dy, dy, dx * dx));
+  const double t = fma(__dsqrt_rn(ss), cfix, dfix);
+  return (uint32_t)__double2loint(__dadd_rn(t, 6755399441055744.0));
+}
+
+constexpr double LEG_LIMIT = 8388608.0;  // 2^23 samples: fixed-point legs and delays stay below it
+
+// Range of |g - c| for c in [c0, c1].
+__device__ __forceinline__ void offset_range(double g, double c0, double c1, double &lo, double &hi) {
+  lo = g < c0 ? c0 - g : (g > c1 ? g - c1 : 0.0);
+  hi = fmax(fabs(g - c0), fabs(g - c1));
+}
+
+// Range of |s(c)| for c in [c0, c1], s the reference's stripe offset: 0 on
+// [e0, e1], e0 - c below, e1 - c above (extra_src/das.cc:470-480).
+__device__ __forceinline__ void stripe_range(double e0, double e1, double c0, double c1, double &lo, double &hi) {
+  auto s = [&](double c) { return (c >= e0 && c <= e1) ? 0.0 : (c < e0 ? e0 - c : e1 - c); };
+  hi = fmax(fabs(s(c0)), fabs(s(c1)));
+  lo = (e0 <= e1) ? fmax(0.0, fmax(e0 - c1, c0 - e1)) : 0.0;
+}
+
+// Bounding box of a tile's image points and delays: x, y, z, delay (ms).
+struct TileBox {
+  double lo[4], hi[4];
+};
+
+// Leg range [Lmin, Lmax] in samples of element e over the tile box.
+__device__ __forceinline__ void leg_range(const FastParams &P, const TileBox &B, bool outer, int e, double &Lmin,
+                                          double &Lmax) {
+  double lx, hx, ly, hy, lz, hz;
+  if (P.method == TFM) {
+    const double *G = outer ? P.Gt : P.Gr;
+    const int N = outer ? P.Nt : P.Nr;
+    offset_range(G[e], B.lo[0], B.hi[0], lx, hx);
+    offset_range(G[e + N], B.lo[1], B.hi[1], ly, hy);
+    offset_range(G[e + 2 * N], B.lo[2], B.hi[2], lz, hz);
+  } else if ((P.method == RCA_COLTX) == outer) {  // a column; stripe edges as pixel_of reads them
+    offset_range(P.Gt[e], B.lo[0], B.hi[0], lx, hx);
+    stripe_range(P.Gr[0 + P.Nt], P.Gr[P.Nt - 1 + P.Nt], B.lo[1], B.hi[1], ly, hy);
+    offset_range(P.Gt[e + 2 * P.Nt], B.lo[2], B.hi[2], lz, hz);
+  } else {  // a row
+    stripe_range(P.Gt[0], P.Gt[P.Nr - 1], B.lo[0], B.hi[0], lx, hx);
+    offset_range(P.Gr[e + P.Nr], B.lo[1], B.hi[1], ly, hy);
+    offset_range(P.Gr[e + 2 * P.Nr], B.lo[2], B.hi[2], lz, hz);
+  }
+  const bool dl = (P.method == RCA_ROWTX) ? !outer : outer;  // the leg that carries the delay
+  Lmin = (sqrt(lx * lx + ly * ly + lz * lz) * P.ocp + (dl ? B.lo[3] : 0.0)) * P.Fs;
+  Lmax = (sqrt(hx * hx + hy * hy + hz * hz) * P.ocp + (dl ? B.hi[3] : 0.0)) * P.Fs;
 }
 
 struct TileShared {
-  int *minA, *maxA, *minB, *maxB;
+  double *red;     // [8 warps][8]: box reduction
+  int *stat;       // [8 warps][8]: classification reduction
+  int *base;       // [n_out + n_in]: integer base of each leg over the tile (outer first)
+  int *ext;        // [n_out + n_in]: bound of (floor(leg) - base)
   uint32_t *ahi;   // [n_out]: high word of the outer legs (column offset + base)
-  uint32_t *arel;  // [n_out][nthreads]
-  int *flags;      // [0]: extent or range failure
+  uint32_t *arel;  // [n_out][nthreads]: outer legs, fixed point relative to base, + delta
+  uint32_t *brel;  // [JC][nthreads]: the current chunk's inner legs, relative to base
 };
 
 // Exact partial sum of terms (o, i0 .. i0+jn-1): every index through the FP64
@@ -201,7 +292,7 @@ __device__ __noinline__ float exact_partial(const FastParams &P, const Pixel &px
   float part = 0.0f;
   for (int j = 0; j < jn; j++) {
     int k;
-    const int64_t col = (int64_t)o * n_in + i0 + j;
+    const int64_t col = ycol(P, n_in, o, i0 + j);
     if (exact_index(P, px, o, i0 + j, k)) {
       const float y = gather_ok<float>(col * P.K + k, y_count(P), P.bad) ? load_sample(Y + col * P.K + k) : 0.0f;
       part = WEIGHTED ? fmaf(__ldg(P.w + col), y, part) : part + y;
@@ -216,7 +307,9 @@ __device__ __noinline__ float exact_partial(const FastParams &P, const Pixel &px
 // chunks, so the unrolled body carries no per-term predicates). Gathers are
 // issued unconditionally: in an in-bounds tile every floor index, ambiguous
 // or not, lies inside its A-scan. Ambiguity is tracked as the minimum
-// fraction word; a chunk whose minimum falls in the band is recomputed.
+// fraction word; a chunk whose minimum falls in the band is recomputed. The
+// minimum runs as four interleaved chains and the packed sums as a tree, so
+// no long dependency chain holds the warp.
 template <class YT, bool WEIGHTED, bool CHECKED, bool FULL, int JC, int NO>
 __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &px, const uint64_t (&B64)[JC],
                                              const uint64_t (&A64)[NO], int o0, int i0, int jn, int n_in,
@@ -225,26 +318,27 @@ __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &p
   // any (rare) call to the exact path, so they are in flight together.
   const YT *__restrict__ Y = reinterpret_cast<const YT *>(P.Y);
   const int64_t K = P.K;
+  constexpr int NM = JC < 4 ? JC : 4;  // independent minimum chains per outer element
   float y[NO][JC];
-  uint32_t minlo[NO];
+  uint32_t mlo[NO][NM];
   unsigned int oob_chunk[NO];
 #pragma unroll
   for (int q = 0; q < NO; q++) {
-    minlo[q] = 0xffffffffu;
     oob_chunk[q] = 0;
+#pragma unroll
+    for (int c = 0; c < NM; c++) mlo[q][c] = 0xffffffffu;
 #pragma unroll
     for (int j = 0; j < JC; j++) {
       y[q][j] = 0.0f;
       if (FULL || j < jn) {
         const uint64_t s = A64[q] + B64[j];
-        const uint32_t lo = (uint32_t)s;
+        mlo[q][j % NM] = min(mlo[q][j % NM], (uint32_t)s);
         const uint32_t off = (uint32_t)(s >> 32);
-        minlo[q] = min(minlo[q], lo);
         if (CHECKED) {
           // Outside the ambiguity band the floor index is exact: [0, K) is in
           // bounds, -1 means p in (-1, 0), i.e. sample 0 after truncation, and
           // anything else is out of bounds.
-          const int64_t col0 = ((int64_t)(o0 + q) * n_in + i0 + j) * K;
+          const int64_t col0 = ycol(P, n_in, o0 + q, i0 + j) * K;
           const int32_t kk = (int32_t)(off - (uint32_t)col0);  // floor index, exact modulo 2^32
           if (kk >= 0 && kk < K) {
             if (gather_ok<float>(col0 + kk, y_count(P), P.bad)) y[q][j] = load_sample(Y + col0 + kk);
@@ -261,11 +355,15 @@ __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &p
   }
   float total = 0.0f;
   float partq[NO];
+  uint32_t minlo[NO];
 #pragma unroll
   for (int q = 0; q < NO; q++) {
+    minlo[q] = mlo[q][0];
+#pragma unroll
+    for (int c = 1; c < NM; c++) minlo[q] = min(minlo[q], mlo[q][c]);
     float part = 0.0f;
     if (WEIGHTED) {
-      const float *w = P.w + (int64_t)(o0 + q) * n_in + i0;
+      const float *w = P.w + ycol(P, n_in, o0 + q, i0);
       if (FULL && ((reinterpret_cast<uintptr_t>(w) & 15) == 0)) {
         uint64_t acc2 = 0;  // (+0, +0)
 #pragma unroll
@@ -281,11 +379,15 @@ __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &p
           if (FULL || j < jn) part = fmaf(__ldg(w + j), y[q][j], part);
       }
     } else {
-      // packed FP32x2 adds: half the instructions and half the dependency depth
-      uint64_t acc2 = pack_f32x2(y[q][0], y[q][1]);
+      // packed FP32x2 adds: half the instructions; summed as a tree
+      uint64_t v[JC / 2];
 #pragma unroll
-      for (int j = 2; j < JC; j += 2) acc2 = add_f32x2(acc2, pack_f32x2(y[q][j], y[q][j + 1]));
-      part = lo_f32(acc2) + hi_f32(acc2);
+      for (int j = 0; j < JC / 2; j++) v[j] = pack_f32x2(y[q][2 * j], y[q][2 * j + 1]);
+#pragma unroll
+      for (int w = JC / 4; w >= 1; w /= 2)
+#pragma unroll
+        for (int j = 0; j < w; j++) v[j] = add_f32x2(v[j], v[j + w]);
+      part = lo_f32(v[0]) + hi_f32(v[0]);
     }
     partq[q] = part;
   }
@@ -304,28 +406,41 @@ __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &p
 
 template <class YT, bool WEIGHTED, bool CHECKED, int JC>
 __device__ __forceinline__ void tile_loop(const FastParams &P, const Pixel &px, const TileShared &S, const FixFmt F,
-                                          int tid,
-                                          int nthr, int n_out, int n_in, int i_lo, int i_hi, float &acc_s,
-                                          float &acc_c, unsigned int &oob) {
+                                          double cfix, double dfixB, int tid, int nthr, int n_out, int n_in,
+                                          int i_lo, int i_hi, float &acc_s, float &acc_c, unsigned int &oob) {
   const int64_t K = P.K;
   for (int i0 = i_lo; i0 < i_hi; i0 += JC) {
     const int jn = min(JC, i_hi - i0);
+    // the chunk's inner legs, one at a time into this thread's shared slots
+    // (computing them side by side in registers would crowd the gather loop)
+    bool bad = false;
+#pragma unroll 1
+    for (int j = 0; j < jn; j++) {
+      const int i = i0 + j;
+      double dx, dy, dz;
+      leg_diffs(P, px, false, i, dx, dy, dz);
+      const uint32_t r = leg_fix(dx, dy, dz, cfix, dfixB) - ((uint32_t)S.base[n_out + i] << F.fb);
+      bad |= r >= ((uint32_t)(S.ext[n_out + i] + 1) << F.fb);
+      S.brel[j * nthr + tid] = r;
+    }
     uint64_t B64[JC];
 #pragma unroll
     for (int j = 0; j < JC; j++) {
       B64[j] = 0;
       if (j < jn) {
         const int i = i0 + j;
-        int fl;
-        bool ok;
-        uint32_t v = fix_leg(A_mul_Fs(P, inner_leg(P, px, i)), F.fb, fl, ok);
-        uint32_t brel = v - ((uint32_t)S.minB[i] << F.fb);
-        uint32_t hi = (uint32_t)(i * K + S.minB[i]);
-        B64[j] = ((uint64_t)brel << F.lo_shift) + ((uint64_t)hi << 32);
+        const uint32_t hi = (uint32_t)(ycol_inner(P, i) * K + S.base[n_out + i]);
+        B64[j] = ((uint64_t)S.brel[j * nthr + tid] << F.lo_shift) + ((uint64_t)hi << 32);
       }
     }
+    if (__any_sync(0xffffffffu, bad)) {
+      // an inner leg outside the tile's bound: this chunk through the exact path
+      for (int o = 0; o < n_out; o++)
+        neumaier(acc_s, acc_c, exact_partial<YT, WEIGHTED>(P, px, o, i0, jn, n_in, oob));
+      continue;
+    }
     if (jn == JC) {
-      // compensation every two outer elements (32 terms)
+      // compensation every two outer elements
       int o = 0;
       for (; o + 2 <= n_out; o += 2) {
         const uint64_t A2[2] = {((uint64_t)S.arel[o * nthr + tid] << F.lo_shift) + ((uint64_t)S.ahi[o] << 32),
@@ -345,32 +460,40 @@ __device__ __forceinline__ void tile_loop(const FastParams &P, const Pixel &px, 
   }
 }
 
-}  // namespace
+// Everything a tile needs before its terms: the image point of each thread,
+// the leg bounds and fixed-point format of the tile, and (unless the tile
+// takes the exact path) the outer legs in shared memory.
+struct TileCtx {
+  Pixel px;
+  int64_t no;
+  bool active, exact_tile, in_bounds;
+  int tid, nthr, n_out, n_in, i_lo, i_hi;
+  FixFmt F;
+  double cfix, dfixB;
+  int ext_outer, ext_inner;  // largest (top - base) of the outer and of the inner legs
+  TileShared S;
+};
 
-// One tile of image points (tile indices tfi along the fast axis, tsi along
-// the slow axis) with the frame described by P; smem_raw holds the tile's
-// shared arrays (fast_smem_bytes). Called by the one-frame kernel and by the
-// persistent batch kernel.
-template <class YT, bool WEIGHTED, int JC>
-__device__ __forceinline__ void fast_tile(const FastParams &P, int64_t tfi, int64_t tsi, unsigned char *smem_raw) {
+__device__ __forceinline__ void tile_setup(const FastParams &P, int64_t tfi, int64_t tsi, unsigned char *smem_raw,
+                                           TileCtx &T) {
   const int tid = threadIdx.x;
   const int nthr = blockDim.x;
-  const int lane = tid & 31, warp = tid >> 5;
+  const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
   const int n_out = (P.method == RCA_ROWTX) ? P.Nr : P.Nt;
   const int n_in = (P.method == RCA_ROWTX) ? P.Nt : P.Nr;
   // inner elements of this launch: all of them unless the caller sets a range
   const int i_lo = P.in_lo, i_hi = P.in_hi > 0 ? P.in_hi : n_in;
 
   TileShared S;
-  S.minA = reinterpret_cast<int *>(smem_raw);
-  S.maxA = S.minA + n_out;
-  S.minB = S.maxA + n_out;
-  S.maxB = S.minB + n_in;
-  S.flags = S.maxB + n_in;
-  S.ahi = reinterpret_cast<uint32_t *>(S.flags + 4);
+  S.red = reinterpret_cast<double *>(smem_raw);
+  S.stat = reinterpret_cast<int *>(S.red + 64);
+  S.base = S.stat + 64;
+  S.ext = S.base + n_out + n_in;
+  S.ahi = reinterpret_cast<uint32_t *>(S.ext + n_out + n_in);
   S.arel = S.ahi + n_out;
+  S.brel = S.arel + n_out * nthr;
 
-  // ---- image point of this thread ----
+  // ---- image point of this thread (inactive lanes repeat the tile's first point) ----
   const int lf = lane % P.wf, ls = lane / P.wf;
   const int warps_f = P.tile_f / P.wf;
   const int wfi = warp % warps_f, wsi = warp / warps_f;
@@ -382,74 +505,168 @@ __device__ __forceinline__ void fast_tile(const FastParams &P, int64_t tfi, int6
   Pixel px;
   pixel_of(P, no, px);
 
-  for (int i = tid; i < n_out; i += nthr) {
-    S.minA[i] = INT_MAX;
-    S.maxA[i] = INT_MIN;
+  // ---- 1. tile box, leg bounds, classification ----
+  {
+    double mn[4] = {px.xo, px.yo, px.zo, px.delay_ms}, mx[4] = {px.xo, px.yo, px.zo, px.delay_ms};
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        mn[q] = fmin(mn[q], __shfl_xor_sync(0xffffffffu, mn[q], off));
+        mx[q] = fmax(mx[q], __shfl_xor_sync(0xffffffffu, mx[q], off));
+      }
+    if (lane == 0)
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        S.red[warp * 8 + q] = mn[q];
+        S.red[warp * 8 + 4 + q] = mx[q];
+      }
   }
-  for (int i = tid; i < n_in; i += nthr) {
-    S.minB[i] = INT_MAX;
-    S.maxB[i] = INT_MIN;
-  }
-  if (tid == 0) S.flags[0] = 0;
   __syncthreads();
-
-  // ---- pass 1: scaled legs, tile-wide integer ranges ----
-  bool bad = false;
-  for (int o = 0; o < n_out; o++) {
-    int fl;
-    bool ok;
-    uint32_t v = fix_leg(A_mul_Fs(P, outer_leg(P, px, o)), FMT_FINE.fb, fl, ok);
-    bad |= !ok;
-    S.arel[o * nthr + tid] = v;
-    int mn = __reduce_min_sync(0xffffffffu, fl), mx = __reduce_max_sync(0xffffffffu, fl);
-    if (lane == 0) {
-      atomicMin(&S.minA[o], mn);
-      atomicMax(&S.maxA[o], mx);
+  TileBox box;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    box.lo[q] = S.red[q];
+    box.hi[q] = S.red[4 + q];
+  }
+  for (int w = 1; w < nwarps; w++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      box.lo[q] = fmin(box.lo[q], S.red[w * 8 + q]);
+      box.hi[q] = fmax(box.hi[q], S.red[w * 8 + 4 + q]);
+    }
+  // delays beyond the fixed-point range send the tile to the exact path
+  int bad = !(fabs(box.lo[3] * P.Fs) < LEG_LIMIT && fabs(box.hi[3] * P.Fs) < LEG_LIMIT);
+  int ext_max = 0, extA = 0, loA = INT_MAX, hiA = INT_MIN, loB = INT_MAX, hiB = INT_MIN;
+  for (int e = tid; e < n_out + n_in; e += nthr) {
+    const bool outer = e < n_out;
+    const int el = outer ? e : e - n_out;
+    if (!outer && (el < i_lo || el >= i_hi)) {
+      S.base[e] = 0;
+      S.ext[e] = 0;
+      continue;
+    }
+    double Lmin, Lmax;
+    leg_range(P, box, outer, el, Lmin, Lmax);
+    int b = 0, t = 0;
+    if (Lmin > -LEG_LIMIT && Lmax < LEG_LIMIT && Lmin <= Lmax) {
+      b = ((int)floor(Lmin) - 1) & ~3;  // a multiple of 4: the scatter's windows start 16-byte aligned
+      t = (int)floor(Lmax) + 1;
+    } else {
+      bad = 1;
+    }
+    S.base[e] = b;
+    S.ext[e] = t - b;
+    ext_max = max(ext_max, t - b);
+    if (outer) extA = max(extA, t - b);
+    if (outer) {
+      loA = min(loA, b);
+      hiA = max(hiA, t);
+    } else {
+      loB = min(loB, b);
+      hiB = max(hiB, t);
     }
   }
-  for (int i = i_lo; i < i_hi; i++) {
-    int fl;
-    bool ok;
-    fix_leg(A_mul_Fs(P, inner_leg(P, px, i)), FMT_FINE.fb, fl, ok);
-    bad |= !ok;
-    int mn = __reduce_min_sync(0xffffffffu, fl), mx = __reduce_max_sync(0xffffffffu, fl);
-    if (lane == 0) {
-      atomicMin(&S.minB[i], mn);
-      atomicMax(&S.maxB[i], mx);
-    }
+  bad = __reduce_or_sync(0xffffffffu, bad);
+  ext_max = __reduce_max_sync(0xffffffffu, ext_max);
+  loA = __reduce_min_sync(0xffffffffu, loA);
+  hiA = __reduce_max_sync(0xffffffffu, hiA);
+  loB = __reduce_min_sync(0xffffffffu, loB);
+  hiB = __reduce_max_sync(0xffffffffu, hiB);
+  extA = __reduce_max_sync(0xffffffffu, extA);
+  if (lane == 0) {
+    S.stat[warp * 8 + 6] = extA;
+    S.stat[warp * 8 + 0] = bad;
+    S.stat[warp * 8 + 1] = ext_max;
+    S.stat[warp * 8 + 2] = loA;
+    S.stat[warp * 8 + 3] = hiA;
+    S.stat[warp * 8 + 4] = loB;
+    S.stat[warp * 8 + 5] = hiB;
   }
-  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&S.flags[0], 1);
   __syncthreads();
-
-  // ---- tile classification (uniform) ----
-  int ext = 0, loA = INT_MAX, hiA = INT_MIN, loB = INT_MAX, hiB = INT_MIN;
-  for (int o = 0; o < n_out; o++) {
-    ext = max(ext, S.maxA[o] - S.minA[o]);
-    loA = min(loA, S.minA[o]);
-    hiA = max(hiA, S.maxA[o]);
+  for (int w = 0; w < nwarps; w++) {
+    bad |= S.stat[w * 8 + 0];
+    ext_max = max(ext_max, S.stat[w * 8 + 1]);
+    loA = min(loA, S.stat[w * 8 + 2]);
+    hiA = max(hiA, S.stat[w * 8 + 3]);
+    loB = min(loB, S.stat[w * 8 + 4]);
+    hiB = max(hiB, S.stat[w * 8 + 5]);
+    extA = max(extA, S.stat[w * 8 + 6]);
   }
-  for (int i = i_lo; i < i_hi; i++) {
-    ext = max(ext, S.maxB[i] - S.minB[i]);
-    loB = min(loB, S.minB[i]);
-    hiB = max(hiB, S.maxB[i]);
-  }
-  const bool exact_tile = S.flags[0] != 0 || ext > WIDE_EXTENT ||
-                          (int64_t)n_out * n_in * P.K + (int64_t)hiA + hiB + 8448 >= (int64_t(1) << 32) ||
-                          (int64_t)loA + loB < -(int64_t(1) << 30);
-  // a non-ambiguous term's floor index lies in [minA + minB, maxA + maxB + 2]
+  const int64_t stride = P.ycol_o > 0 ? P.ycol_o : n_in;
+  bool exact_tile = bad || ext_max > WIDE_EXTENT || loA > hiA ||
+                    (int64_t)n_out * stride * P.K + (int64_t)hiA + hiB + 8448 >= (int64_t(1) << 32) ||
+                    (int64_t)loA + loB < -(int64_t(1) << 30);
+  // a non-ambiguous term's floor index lies in [loA + loB, hiA + hiB + 2]
   const bool in_bounds = (int64_t)loA + loB >= 0 && (int64_t)hiA + hiB + 2 < P.K;
 
+  const FixFmt F = ext_max > FINE_EXTENT ? FMT_WIDE : FMT_FINE;
+  const double scale = (double)(1u << F.fb);
+  const double cfix = P.ocp * P.Fs * scale;
+  const double dfix = px.delay_ms * P.Fs * scale;
+  if (!exact_tile) {
+    // ---- 2. outer legs, relative to their bases, plus the delta shift ----
+    int leg_bad = 0;
+    for (int o = 0; o < n_out; o++) {
+      double dx, dy, dz;
+      leg_diffs(P, px, true, o, dx, dy, dz);
+      const uint32_t r = leg_fix(dx, dy, dz, cfix, P.method == RCA_ROWTX ? 0.0 : dfix) - ((uint32_t)S.base[o] << F.fb);
+      leg_bad |= r >= ((uint32_t)(S.ext[o] + 1) << F.fb);
+      S.arel[o * nthr + tid] = r + F.delta;
+    }
+    for (int o = tid; o < n_out; o += nthr) S.ahi[o] = (uint32_t)(ycol_outer(P, n_in, o) * P.K + S.base[o]);
+    exact_tile = __syncthreads_or(leg_bad) != 0;
+  }
+  T.px = px;
+  T.no = no;
+  T.active = active;
+  T.exact_tile = exact_tile;
+  T.in_bounds = in_bounds;
+  T.tid = tid;
+  T.nthr = nthr;
+  T.n_out = n_out;
+  T.n_in = n_in;
+  T.i_lo = i_lo;
+  T.i_hi = i_hi;
+  T.F = F;
+  T.cfix = cfix;
+  T.dfixB = P.method == RCA_ROWTX ? dfix : 0.0;
+  T.ext_outer = extA;
+  T.ext_inner = 0;
+  for (int e = n_out + i_lo; e < n_out + i_hi; e++) T.ext_inner = max(T.ext_inner, S.ext[e]);
+  T.S = S;
+}
+
+}  // namespace
+
+// One tile of image points (tile indices tfi along the fast axis, tsi along
+// the slow axis) with the frame described by P; smem_raw holds the tile's
+// shared arrays (fast_smem_bytes). Called by the one-frame kernel and by the
+// persistent batch kernel.
+//
+// 1. The box bounding the tile's points and delays gives every element's leg
+//    range over the tile (leg_range): an integer base and extent per leg,
+//    and the tile's fixed-point format.
+// 2. Each point's outer legs are converted once (leg_fix) into shared memory,
+//    relative to their bases; each inner leg is converted once per point in
+//    the main loop. A leg outside its bound (which the box bound rules out up
+//    to rounding) sends its tile (outer) or chunk (inner) to the exact path
+//    before any gather depends on it.
+template <class YT, bool WEIGHTED, int JC>
+__device__ __forceinline__ void fast_tile(const FastParams &P, int64_t tfi, int64_t tsi, unsigned char *smem_raw) {
+  TileCtx T;
+  tile_setup(P, tfi, tsi, smem_raw, T);
   float acc_s = 0.0f, acc_c = 0.0f;
   unsigned int oob = 0;
   const YT *__restrict__ Yp = reinterpret_cast<const YT *>(P.Y);
-  if (exact_tile) {
+  if (T.exact_tile) {
     // every term through the exact FP64 index
-    for (int o = 0; o < n_out; o++) {
+    for (int o = 0; o < T.n_out; o++) {
       float part = 0.0f;
-      for (int i = i_lo; i < i_hi; i++) {
+      for (int i = T.i_lo; i < T.i_hi; i++) {
         int k;
-        const int64_t col = (int64_t)o * n_in + i;
-        if (exact_index(P, px, o, i, k)) {
+        const int64_t col = ycol(P, T.n_in, o, i);
+        if (exact_index(P, T.px, o, i, k)) {
           float y = load_sample(Yp + col * P.K + k);
           part = WEIGHTED ? fmaf(__ldg(P.w + col), y, part) : part + y;
         } else {
@@ -458,32 +675,19 @@ __device__ __forceinline__ void fast_tile(const FastParams &P, int64_t tfi, int6
       }
       neumaier(acc_s, acc_c, part);
     }
+  } else if (T.in_bounds) {
+    tile_loop<YT, WEIGHTED, false, JC>(P, T.px, T.S, T.F, T.cfix, T.dfixB, T.tid, T.nthr, T.n_out, T.n_in, T.i_lo,
+                                       T.i_hi, acc_s, acc_c, oob);
   } else {
-    // format of this tile; rebase the outer legs on the tile minimum and add
-    // the delta shift (the wide format converts the outer legs again)
-    const FixFmt F = ext > FINE_EXTENT ? FMT_WIDE : FMT_FINE;
-    for (int o = 0; o < n_out; o++) {
-      uint32_t v = S.arel[o * nthr + tid];
-      if (F.fb != FMT_FINE.fb) {
-        int fl;
-        bool ok;
-        v = fix_leg(A_mul_Fs(P, outer_leg(P, px, o)), F.fb, fl, ok);
-      }
-      S.arel[o * nthr + tid] = v - ((uint32_t)S.minA[o] << F.fb) + F.delta;
-    }
-    for (int o = tid; o < n_out; o += nthr) S.ahi[o] = (uint32_t)((int64_t)o * n_in * P.K + S.minA[o]);
-    __syncthreads();
-    if (in_bounds)
-      tile_loop<YT, WEIGHTED, false, JC>(P, px, S, F, tid, nthr, n_out, n_in, i_lo, i_hi, acc_s, acc_c, oob);
-    else
-      tile_loop<YT, WEIGHTED, true, JC>(P, px, S, F, tid, nthr, n_out, n_in, i_lo, i_hi, acc_s, acc_c, oob);
+    tile_loop<YT, WEIGHTED, true, JC>(P, T.px, T.S, T.F, T.cfix, T.dfixB, T.tid, T.nthr, T.n_out, T.n_in, T.i_lo,
+                                      T.i_hi, acc_s, acc_c, oob);
   }
-  if (active) P.Im[no] = P.accumulate ? P.Im[no] + (acc_s + acc_c) : acc_s + acc_c;
-  add_count(P.oob, active ? oob : 0u);
+  if (T.active) P.Im[T.no] = P.accumulate ? P.Im[T.no] + (acc_s + acc_c) : acc_s + acc_c;
+  add_count(P.oob, T.active ? oob : 0u);
 }
 
 template <class YT, bool WEIGHTED, int JC>
-__global__ void __launch_bounds__(256) das_fast_kernel(const FastParams P) {
+__global__ void __launch_bounds__(256, 2) das_fast_kernel(const FastParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   fast_tile<YT, WEIGHTED, JC>(P, blockIdx.x, (int64_t)blockIdx.y + P.slow_tile0, smem_raw);
 }
@@ -493,7 +697,7 @@ __global__ void __launch_bounds__(256) das_fast_kernel(const FastParams P) {
 // descriptor is staged in shared memory; every frame's tile has blockDim.x
 // points. ctr must be zero at launch (the batch run resets it).
 template <class YT>
-__global__ void __launch_bounds__(128) das_batch_kernel(const FastParams *__restrict__ frames,
+__global__ void __launch_bounds__(128, 4) das_batch_kernel(const FastParams *__restrict__ frames,
                                                         const int4 *__restrict__ items, int n_items,
                                                         int *__restrict__ ctr) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -559,7 +763,7 @@ __global__ void f32_to_bf16_kernel(const float *__restrict__ x, __nv_bfloat16 *_
 size_t fast_smem_bytes(const FastParams &P, int nthr) {
   const int n_out = (P.method == RCA_ROWTX) ? P.Nr : P.Nt;
   const int n_in = (P.method == RCA_ROWTX) ? P.Nt : P.Nr;
-  return (size_t)(3 * n_out + 2 * n_in + 4) * sizeof(int) + (size_t)n_out * nthr * sizeof(uint32_t);
+  return fast_smem_bytes_dev(P, n_out, n_in, nthr);
 }
 
 template <class YT, bool W>
@@ -644,348 +848,312 @@ cudaError_t convert_f32_to_bf16(const float *x, void *y, int64_t n, cudaStream_t
 
 
 // ===========================================================================
-// Geometry-bound operator: leg tables, weighted gather, adjoint scatter and
-// weight gradient (the differentiable beamformer and its CG solver).
-//
-// Leg tables hold, per (element, image point), the scaled FP64 leg as 32.32
-// fixed point with the A-scan column offset folded into the high word:
-//   TA[o][n] = (o*n_in*K << 32) + round(A(n,o) * 2^32) + delta
-//   TB[i][n] = (i*K << 32)      + round(B(n,i) * 2^32)
-// so TA + TB has the sample's element offset in its high word and the
-// fraction (shifted by delta) in its low word, exactly as in the tile kernel;
-// the same ambiguity band sends the rare boundary terms to the FP64 path, so
-// all three operators use the FP64 reference indices.
+// Adjoint (scatter) on pixel tiles: Ya[k(n,c), c] += w[c] * x[n] for the
+// tile's image points n and every A-scan column c, at the forward's indices
+// (fixed-point floors outside the ambiguity band, the FP64 chain inside it).
+// Each term is added with a global reduction; the 32 lanes of a warp hit one
+// column at nearby samples, so a warp's reductions fall on a few sectors.
+// Ya must be zeroed (or hold the partial sum to add to) before the launch.
 // ===========================================================================
 
 namespace {
 
-constexpr uint32_t TAB_DELTA = 1u << 10;       // 2^-22 in 2^-32 units
-constexpr uint32_t TAB_AMB_LO = 2 * TAB_DELTA;  // ambiguity band of the table terms
-
-__global__ void legtab_kernel(const FastParams P, int64_t *__restrict__ TA, int64_t *__restrict__ TB,
-                              int *__restrict__ range) {
-  const int n_out = (P.method == RCA_ROWTX) ? P.Nr : P.Nt;
-  const int n_in = (P.method == RCA_ROWTX) ? P.Nt : P.Nr;
-  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int e = blockIdx.y;  // element: [0, n_out) outer, [n_out, n_out+n_in) inner
-  const bool active = n < P.No;
-  Pixel px;
-  pixel_of(P, active ? n : 0, px);
-  const bool outer = e < n_out;
-  const double L = outer ? A_mul_Fs(P, outer_leg(P, px, e)) : A_mul_Fs(P, inner_leg(P, px, e - n_out));
-  const bool ok = fabs(L) < 67108864.0;  // 2^26, as the tile kernel
-  const double f = floor(ok ? L : 0.0);
-  const int fl = (int)f;
-  const uint64_t frac = (uint64_t)__double2ull_rn((ok ? (L - f) : 0.0) * 4294967296.0);  // [0, 2^32]
-  const int64_t colk = outer ? (int64_t)e * n_in * P.K : (int64_t)(e - n_out) * P.K;
-  const int64_t v = ((colk + fl) << 32) + (int64_t)frac + (outer ? TAB_DELTA : 0);
-  if (active) {
-    if (outer) TA[(int64_t)e * P.No + n] = v;
-    else TB[(int64_t)(e - n_out) * P.No + n] = v;
-  }
-  // range[0..3]: min/max floor of outer legs, min/max of inner; [4]: overflow
-  int mn = __reduce_min_sync(0xffffffffu, active ? fl : INT_MAX);
-  int mx = __reduce_max_sync(0xffffffffu, active ? fl : INT_MIN);
-  bool bad = __any_sync(0xffffffffu, active && !ok);
-  if ((threadIdx.x & 31) == 0) {
-    atomicMin(&range[outer ? 0 : 2], mn);
-    atomicMax(&range[outer ? 1 : 3], mx);
-    if (bad) atomicOr(&range[4], 1);
+// Exact scatter of terms (o, i0 .. i0+jn-1) of one image point.
+template <bool WEIGHTED>
+__device__ __noinline__ void exact_scatter(const FastParams &P, const Pixel &px, int o, int i0, int jn, int n_in,
+                                           float xn, float *Ya) {
+  for (int j = 0; j < jn; j++) {
+    int k;
+    const int64_t col = ycol(P, n_in, o, i0 + j);
+    if (exact_index(P, px, o, i0 + j, k)) atomicAdd(Ya + col * P.K + k, WEIGHTED ? __ldg(P.w + col) * xn : xn);
   }
 }
 
-__global__ void legtab_classify_kernel(int *__restrict__ range, int64_t K, int64_t ny) {
-  // range[5] = 1: every non-ambiguous floor index lies in [0, K);
-  // range[6] = 1: element offsets fit 32 bits
-  const int64_t lo = (int64_t)range[0] + range[2], hi = (int64_t)range[1] + range[3];
-  range[5] = (range[4] == 0 && lo >= 0 && hi + 2 < K) ? 1 : 0;
-  range[6] = (range[4] == 0 && ny + hi + 256 < (int64_t(1) << 32) && lo > -(int64_t(1) << 30)) ? 1 : 0;
-}
-
-// Weighted gather Im[n] = sum_c w[c] Y[k(n,c), c] from the leg tables.
-template <class YT, bool WEIGHTED, bool CHECKED, int JC>
-__device__ __forceinline__ void tab_gather_body(const FastParams &P, const Pixel &px, const int64_t *TA,
-                                                const int64_t *TB, int64_t n, int n_out, int n_in,
-                                                float &acc_s, float &acc_c, unsigned int &oob) {
-  for (int i0 = 0; i0 < n_in; i0 += JC) {
-    const int jn = min(JC, n_in - i0);
+template <bool WEIGHTED, bool CHECKED, int JC>
+__device__ __forceinline__ void scatter_loop(const FastParams &P, const TileCtx &T, float xn, float *Ya) {
+  const int64_t K = P.K;
+  const TileShared &S = T.S;
+  const FixFmt F = T.F;
+  const int tid = T.tid, nthr = T.nthr, n_out = T.n_out, n_in = T.n_in;
+  for (int i0 = T.i_lo; i0 < T.i_hi; i0 += JC) {
+    const int jn = min(JC, T.i_hi - i0);
+    bool bad = false;
+#pragma unroll 1
+    for (int j = 0; j < jn; j++) {
+      const int i = i0 + j;
+      double dx, dy, dz;
+      leg_diffs(P, T.px, false, i, dx, dy, dz);
+      const uint32_t r = leg_fix(dx, dy, dz, T.cfix, T.dfixB) - ((uint32_t)S.base[n_out + i] << F.fb);
+      bad |= r >= ((uint32_t)(S.ext[n_out + i] + 1) << F.fb);
+      S.brel[j * nthr + tid] = r;
+    }
+    if (__any_sync(0xffffffffu, bad)) {
+      if (T.active)
+        for (int o = 0; o < n_out; o++) exact_scatter<WEIGHTED>(P, T.px, o, i0, jn, n_in, xn, Ya);
+      continue;
+    }
     uint64_t B64[JC];
 #pragma unroll
-    for (int j = 0; j < JC; j++) B64[j] = (j < jn) ? (uint64_t)__ldg(TB + (int64_t)(i0 + j) * P.No + n) : 0;
+    for (int j = 0; j < JC; j++) {
+      B64[j] = 0;
+      if (j < jn) {
+        const uint32_t hi = (uint32_t)(ycol_inner(P, i0 + j) * K + S.base[n_out + i0 + j]);
+        B64[j] = ((uint64_t)S.brel[j * nthr + tid] << F.lo_shift) + ((uint64_t)hi << 32);
+      }
+    }
     for (int o = 0; o < n_out; o++) {
-      const uint64_t A1[1] = {(uint64_t)__ldg(TA + (int64_t)o * P.No + n)};
-      float part =
-          (jn == JC) ? chunk_terms<YT, WEIGHTED, CHECKED, true, JC, 1>(P, px, B64, A1, o, i0, JC, n_in, TAB_AMB_LO, oob)
-                     : chunk_terms<YT, WEIGHTED, CHECKED, false, JC, 1>(P, px, B64, A1, o, i0, jn, n_in, TAB_AMB_LO, oob);
-      neumaier(acc_s, acc_c, part);
-    }
-  }
-}
-
-template <class YT, bool WEIGHTED>
-__global__ void __launch_bounds__(256) tab_gather_kernel(const FastParams P, const int64_t *__restrict__ TA,
-                                                         const int64_t *__restrict__ TB,
-                                                         const int *__restrict__ range) {
-  const int n_out = (P.method == RCA_ROWTX) ? P.Nr : P.Nt;
-  const int n_in = (P.method == RCA_ROWTX) ? P.Nt : P.Nr;
-  const int64_t n_raw = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool active = n_raw < P.No;
-  const int64_t n = active ? n_raw : 0;
-  Pixel px;
-  pixel_of(P, n, px);
-  float acc_s = 0.0f, acc_c = 0.0f;
-  unsigned int oob = 0;
-  const bool exact_all = range[6] == 0;
-  if (exact_all) {
-    for (int o = 0; o < n_out; o++) {
-      for (int i0 = 0; i0 < n_in; i0 += 16)
-        neumaier(acc_s, acc_c, exact_partial<YT, WEIGHTED>(P, px, o, i0, min(16, n_in - i0), n_in, oob));
-    }
-  } else if (range[5]) {
-    tab_gather_body<YT, WEIGHTED, false, 16>(P, px, TA, TB, n, n_out, n_in, acc_s, acc_c, oob);
-  } else {
-    tab_gather_body<YT, WEIGHTED, true, 16>(P, px, TA, TB, n, n_out, n_in, acc_s, acc_c, oob);
-  }
-  if (active) P.Im[n] = acc_s + acc_c;
-  add_count(P.oob, active ? oob : 0u);
-}
-
-// The term's sample index for the column-owner kernels: returns -1 when the
-// term is out of bounds. Outside the ambiguity band the floor index decides
-// (-1 is p in (-1, 0): sample 0); inside it the FP64 index is recomputed, the
-// only place that needs the image point's coordinates.
-__device__ __noinline__ int tab_index_exact(const FastParams &P, int64_t n, int o, int i) {
-  Pixel px;
-  pixel_of(P, n, px);
-  int k;
-  return exact_index(P, px, o, i, k) ? k : -1;
-}
-
-__device__ __forceinline__ int floor_index(uint64_t s, uint32_t colk, int64_t K) {
-  const int32_t kk = (int32_t)((uint32_t)(s >> 32) - colk);
-  return (kk >= 0 && kk < K) ? kk : (kk == -1 ? 0 : -1);
-}
-
-// Column-owner terms of one image point whose leg sums include an ambiguous
-// one: every term goes through tab_index (floor outside the band, FP64
-// inside). Kept out of line so that the common path holds its arrays in
-// registers. The weight-gradient partials go to the shared accumulator wacc.
-template <bool ADJ, bool WG>
-__device__ __noinline__ void colowner_point_exact(const FastParams &P, const int64_t *__restrict__ TA,
-                                                  const int64_t *__restrict__ TB, int64_t n, int o, int i0, int jn,
-                                                  int n_in, float xn, float gn, float *hist, float *wacc) {
-  const uint64_t A64 = (uint64_t)__ldg(TA + (int64_t)o * P.No + n);
-  const float *Yf = reinterpret_cast<const float *>(P.Y);
-  for (int j = 0; j < jn; j++) {
-    const int64_t col = (int64_t)o * n_in + i0 + j;
-    const uint64_t s = A64 + (uint64_t)__ldg(TB + (int64_t)(i0 + j) * P.No + n);
-    const int k = ((uint32_t)s >= TAB_AMB_LO) ? floor_index(s, (uint32_t)(col * P.K), P.K) : tab_index_exact(P, n, o, i0 + j);
-    if (k < 0) continue;
-    if (ADJ) atomicAdd(hist + (int64_t)j * P.K + k, (P.w ? __ldg(P.w + col) : 1.0f) * xn);
-    if (WG) atomicAdd(wacc + j, gn * __ldg(Yf + col * P.K + k));
-  }
-}
-
-// Column-owner adjoint and weight gradient. A CTA owns outer element o and
-// inner elements [i0, i0 + jn) (jn <= CW), loops over a share of the image
-// points, PX points per thread per step, and
-//   adjoint: Ya[k(n,c), c] += w[c] * X[n]   (shared-memory histogram per column)
-//   wgrad:   dW[c] += G[n] * Y[k(n,c), c]  (per-thread partials, block reduction)
-// The leg-table loads of the PX points are all issued before any index is
-// formed; an image point with an ambiguous term is handed whole to
-// colowner_point_exact.
-template <bool ADJ, bool WG, int CW, int PX>
-__global__ void __launch_bounds__(256, ADJ ? 4 : 3) tab_colowner_kernel(const FastParams P, const int64_t *__restrict__ TA,
-                                                           const int64_t *__restrict__ TB,
-                                                           const float *__restrict__ X, const float *__restrict__ G,
-                                                           float *__restrict__ Ya, float *__restrict__ dW, int splits) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int n_in = (P.method == RCA_ROWTX) ? P.Nt : P.Nr;
-  const int jmax = min(CW, n_in);
-  float *hist = reinterpret_cast<float *>(smem_raw);      // [jmax][K] (adjoint)
-  float *red = hist + (ADJ ? (size_t)jmax * P.K : 0);     // [CW][warps] (wgrad)
-  float *wacc = red + (WG ? CW * (blockDim.x >> 5) : 0);  // [CW] (wgrad, exact points)
-  const int o = blockIdx.x;
-  const int i0 = blockIdx.y * CW;
-  const int jn = min(CW, n_in - i0);
-  const int split = blockIdx.z;
-  const int tid = threadIdx.x, nthr = blockDim.x;
-  const int64_t K = P.K;
-  const float *Yf = reinterpret_cast<const float *>(P.Y);
-  if (ADJ) {
-    for (int64_t q = tid; q < (int64_t)jn * K; q += nthr) hist[q] = 0.0f;
-  }
-  if (WG && tid < CW) wacc[tid] = 0.0f;
-  __syncthreads();
-  float wc[CW];
-  uint32_t colk[CW];
-  float wsum[CW];
+      const uint64_t A64 = ((uint64_t)S.arel[o * nthr + tid] << F.lo_shift) + ((uint64_t)S.ahi[o] << 32);
+      uint64_t sj[JC];
+      uint32_t m = 0xffffffffu;
 #pragma unroll
-  for (int j = 0; j < CW; j++) {
-    const int64_t col = (int64_t)o * n_in + i0 + j;
-    wc[j] = (ADJ && j < jn) ? (P.w ? __ldg(P.w + col) : 1.0f) : 0.0f;
-    colk[j] = (uint32_t)(col * K);
-    wsum[j] = 0.0f;
-  }
-  const int64_t per = (P.No + splits - 1) / splits;
-  const int64_t n0 = (int64_t)split * per, n1 = min(P.No, n0 + per);
-  const int64_t *ta = TA + (int64_t)o * P.No;
-  const int64_t *tb = TB + (int64_t)i0 * P.No;
-  for (int64_t nb = n0 + tid; nb < n1; nb += (int64_t)PX * nthr) {
-    uint64_t s[PX][CW];
-    float xn[PX], gn[PX];
-    bool on[PX];
+      for (int j = 0; j < JC; j++) {
+        sj[j] = A64 + B64[j];
+        if (j < jn) m = min(m, (uint32_t)sj[j]);
+      }
+      if (m < F.amb_lo) {  // an ambiguous term: this outer element's chunk through the exact indices
+        if (T.active) exact_scatter<WEIGHTED>(P, T.px, o, i0, jn, n_in, xn, Ya);
+        continue;
+      }
+      const int64_t colo = ycol_outer(P, n_in, o);
 #pragma unroll
-    for (int q = 0; q < PX; q++) {
-      const int64_t n = nb + (int64_t)q * nthr;
-      on[q] = n < n1;
-      const int64_t nn = on[q] ? n : n0;
-      const uint64_t A64 = (uint64_t)__ldg(ta + nn);
-      xn[q] = ADJ ? __ldg(X + nn) : 0.0f;
-      gn[q] = WG ? __ldg(G + nn) : 0.0f;
-#pragma unroll
-      for (int j = 0; j < CW; j++) s[q][j] = (j < jn) ? A64 + (uint64_t)__ldg(tb + (int64_t)j * P.No + nn) : ~0ull;
-    }
-#pragma unroll
-    for (int q = 0; q < PX; q++) {
-      if (!on[q]) continue;
-      uint32_t minlo = 0xffffffffu;
-#pragma unroll
-      for (int j = 0; j < CW; j++) minlo = min(minlo, (uint32_t)s[q][j]);
-      if (minlo >= TAB_AMB_LO) {
-        int k[CW];
-#pragma unroll
-        for (int j = 0; j < CW; j++) k[j] = (j < jn) ? floor_index(s[q][j], colk[j], K) : -1;
-        if (WG) {
-          float yv[CW];
-#pragma unroll
-          for (int j = 0; j < CW; j++) yv[j] = (k[j] >= 0) ? __ldg(Yf + ((int64_t)o * n_in + i0 + j) * K + k[j]) : 0.0f;
-#pragma unroll
-          for (int j = 0; j < CW; j++) wsum[j] = fmaf(gn[q], yv[j], wsum[j]);
+      for (int j = 0; j < JC; j++) {
+        if (j < jn && T.active) {
+          const float v = WEIGHTED ? __ldg(P.w + colo + ycol_inner(P, i0 + j)) * xn : xn;
+          const uint32_t off = (uint32_t)(sj[j] >> 32);
+          if (CHECKED) {
+            const int64_t col0 = (colo + ycol_inner(P, i0 + j)) * K;
+            const int32_t kk = (int32_t)(off - (uint32_t)col0);
+            if (kk >= 0 && kk < K) atomicAdd(Ya + col0 + kk, v);
+            else if (kk == -1) atomicAdd(Ya + col0, v);
+          } else {
+            atomicAdd(Ya + off, v);
+          }
         }
-        if (ADJ) {
-          const float xq = xn[q];
+      }
+    }
+  }
+}
+
+
+// Columns per shared-memory window batch and samples per window (windows
+// wider than this send their tile to the direct-reduction path).
+constexpr int SCATTER_WCAP = 256;
+
+__device__ __forceinline__ void red_add_v4(float *p, float4 v) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
+               : "memory");
+}
+
+// Window scatter of one tile: for outer element o and a chunk of inner
+// elements, every term goes into the shared-memory window of its column (the
+// tile's sample range [base_o + base_i, ... + WS), 16-byte aligned because the
+// bases are multiples of 4); then the windows are added to Ya with 4-wide
+// vector reductions (the weight applied once per sample) and cleared. Two
+// block barriers per (o, chunk). A term's slot is the high word of A64 + B64
+// when both hold only the relative legs. The windows hold fixed-point
+// integers, x scaled by 2^(22 - E) with max |x| over the tile below 2^E, so
+// the shared-memory additions are native integer atomics, exact and
+// independent of their order (a slot receives at most one term per thread
+// per batch, at most 256 terms of magnitude up to 2^22); each value is
+// rounded once, to within 2^-22 of the tile's largest |x|.
+template <bool WEIGHTED, bool CHECKED, int JC>
+__device__ __forceinline__ void scatter_window_loop(const FastParams &P, const TileCtx &T, float xn_f, float *Ya,
+                                                    float *winf, int WS) {
+  int *win = reinterpret_cast<int *>(winf);
+  const int64_t K = P.K;
+  const TileShared &S = T.S;
+  const FixFmt F = T.F;
+  const int tid = T.tid, nthr = T.nthr, n_out = T.n_out, n_in = T.n_in;
+  const bool vec = !CHECKED && ((K & 3) == 0) && ((reinterpret_cast<uintptr_t>(Ya) & 15) == 0);
+  // fixed-point scale of the tile: max |x| < 2^E, values scaled by 2^(22 - E)
+  float mx = fabsf(xn_f);
+  for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+  __shared__ float s_mx[8];
+  if ((tid & 31) == 0) s_mx[tid >> 5] = mx;
+  for (int e = tid; e < JC * WS; e += nthr) win[e] = 0;
+  __syncthreads();
+  mx = 0.0f;
+  for (int w = 0; w < (nthr >> 5); w++) mx = fmaxf(mx, s_mx[w]);
+  if (mx == 0.0f) return;  // nothing to add
+  int E;
+  frexpf(mx, &E);
+  const float qscale = ldexpf(1.0f, 22 - E), iS = ldexpf(1.0f, E - 22);
+  const int xn = __float2int_rn(xn_f * qscale);
+  for (int i0 = T.i_lo; i0 < T.i_hi; i0 += JC) {
+    const int jn = min(JC, T.i_hi - i0);
+    bool bad = false;
+#pragma unroll 4
+    for (int j = 0; j < jn; j++) {
+      const int i = i0 + j;
+      double dx, dy, dz;
+      leg_diffs(P, T.px, false, i, dx, dy, dz);
+      const uint32_t r = leg_fix(dx, dy, dz, T.cfix, T.dfixB) - ((uint32_t)S.base[n_out + i] << F.fb);
+      bad |= r >= ((uint32_t)(S.ext[n_out + i] + 1) << F.fb);
+      S.brel[j * nthr + tid] = r;
+    }
+    if (__syncthreads_or(bad)) {
+      // an inner leg outside the tile's bound: this chunk through the exact indices, straight to Ya
+      if (T.active)
+        for (int o = 0; o < n_out; o++) exact_scatter<WEIGHTED>(P, T.px, o, i0, jn, n_in, xn_f, Ya);
+      continue;
+    }
+    uint64_t B64[JC];
 #pragma unroll
-          for (int j = 0; j < CW; j++)
-            if (k[j] >= 0) atomicAdd(hist + j * K + k[j], wc[j] * xq);
+    for (int j = 0; j < JC; j++) B64[j] = (j < jn) ? ((uint64_t)S.brel[j * nthr + tid] << F.lo_shift) : 0;
+    for (int o = 0; o < n_out; o++) {
+      const uint64_t A64 = (uint64_t)S.arel[o * nthr + tid] << F.lo_shift;
+      uint64_t sj[JC];
+      uint32_t m = 0xffffffffu;
+#pragma unroll
+      for (int j = 0; j < JC; j++) {
+        sj[j] = A64 + B64[j];
+        if (j < jn) m = min(m, (uint32_t)sj[j]);
+      }
+      if (T.active) {
+        if (m < F.amb_lo) {
+          // an ambiguous term: this outer element's chunk at the exact indices
+          for (int j = 0; j < jn; j++) {
+            int k;
+            if (exact_index(P, T.px, o, i0 + j, k)) {
+              const int slot = k - (S.base[o] + S.base[n_out + i0 + j]);
+              if (slot >= 0 && slot < WS) atomicAdd(win + j * WS + slot, xn);
+              else atomicAdd(Ya + ycol(P, n_in, o, i0 + j) * K + k, WEIGHTED ? __ldg(P.w + ycol(P, n_in, o, i0 + j)) * xn_f : xn_f);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < JC; j++)
+            if (j < jn) atomicAdd(win + j * WS + (int)(sj[j] >> 32), xn);
+        }
+      }
+      __syncthreads();
+      const int64_t colo = ycol_outer(P, n_in, o);
+      if (vec) {
+        const int w4 = WS >> 2;
+        for (int e = tid; e < jn * w4; e += nthr) {
+          const int j = e / w4, t4 = (e - j * w4) << 2;
+          int4 *wp = reinterpret_cast<int4 *>(win + j * WS + t4);
+          const int4 vi = *wp;
+          *wp = make_int4(0, 0, 0, 0);
+          if (vi.x | vi.y | vi.z | vi.w) {
+            float4 v = make_float4((float)vi.x * iS, (float)vi.y * iS, (float)vi.z * iS, (float)vi.w * iS);
+            const int64_t col = colo + ycol_inner(P, i0 + j);
+            const int64_t k0 = (int64_t)S.base[o] + S.base[n_out + i0 + j] + t4;  // a multiple of 4
+            if (WEIGHTED) {
+              const float wc = __ldg(P.w + col);
+              v.x *= wc;
+              v.y *= wc;
+              v.z *= wc;
+              v.w *= wc;
+            }
+            if (k0 >= 0 && k0 + 4 <= K) {
+              red_add_v4(Ya + col * K + k0, v);
+            } else {  // a window edge beyond the A-scan holds only zeros; added one by one to stay inside
+              const float vv[4] = {v.x, v.y, v.z, v.w};
+              for (int q = 0; q < 4; q++)
+                if (vv[q] != 0.0f && k0 + q >= 0 && k0 + q < K) atomicAdd(Ya + col * K + k0 + q, vv[q]);
+            }
+          }
         }
       } else {
-        colowner_point_exact<ADJ, WG>(P, TA, TB, nb + (int64_t)q * nthr, o, i0, jn, n_in, xn[q], gn[q], hist, wacc);
+        for (int e = tid; e < jn * WS; e += nthr) {
+          const int j = e / WS, t = e - j * WS;
+          const float v = (float)win[e] * iS;
+          win[e] = 0;
+          if (v != 0.0f) {
+            const int64_t col = colo + ycol_inner(P, i0 + j);
+            int64_t k = (int64_t)S.base[o] + S.base[n_out + i0 + j] + t;
+            if (k == -1) k = 0;  // p in (-1, 0): sample 0 after truncation toward zero
+            if (k >= 0 && k < K) atomicAdd(Ya + col * K + k, WEIGHTED ? __ldg(P.w + col) * v : v);
+          }
+        }
       }
+      __syncthreads();
     }
   }
+}
+
+template <bool WEIGHTED, int JC>
+__global__ void __launch_bounds__(256, 2) das_scatter_kernel(const FastParams P, const float *__restrict__ X,
+                                                             float *__restrict__ Ya) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TileCtx T;
+  tile_setup(P, blockIdx.x, (int64_t)blockIdx.y + P.slow_tile0, smem_raw, T);
+  const float xn = T.active ? __ldg(X + T.no) : 0.0f;
+  const int WS = (T.ext_outer + T.ext_inner + 4 + 3) & ~3;  // window samples per column
+  float *win = reinterpret_cast<float *>(smem_raw + fast_smem_bytes_dev(P, T.n_out, T.n_in, T.nthr));
+  if (!T.exact_tile && WS <= SCATTER_WCAP) {
+    if (T.in_bounds) scatter_window_loop<WEIGHTED, false, JC>(P, T, xn, Ya, win, WS);
+    else scatter_window_loop<WEIGHTED, true, JC>(P, T, xn, Ya, win, WS);
+  } else if (T.exact_tile) {
+    if (T.active)
+      for (int o = 0; o < T.n_out; o++)
+        for (int i0 = T.i_lo; i0 < T.i_hi; i0 += 16)
+          exact_scatter<WEIGHTED>(P, T.px, o, i0, min(16, T.i_hi - i0), T.n_in, xn, Ya);
+  } else if (T.in_bounds) {
+    scatter_loop<WEIGHTED, false, JC>(P, T, xn, Ya);
+  } else {
+    scatter_loop<WEIGHTED, true, JC>(P, T, xn, Ya);
+  }
+}
+
+}  // namespace
+
+// Tile scatter over the same tiles and slow-tile ranges as launch_fast (P as
+// for the forward; P.w optional). Ya is not zeroed here.
+cudaError_t launch_scatter(const FastParams &P, const float *X, float *Ya, cudaStream_t st) {
+  const int nthr = P.tile_f * P.tile_s;
+  // the tile's arrays, then the windows of one (outer, inner chunk) batch
+  const size_t smem = fast_smem_bytes(P, nthr) + (size_t)(P.jc == 8 ? 8 : 16) * SCATTER_WCAP * sizeof(float);
+  auto kern = P.w ? (P.jc == 8 ? das_scatter_kernel<true, 8> : das_scatter_kernel<true, 16>)
+                  : (P.jc == 8 ? das_scatter_kernel<false, 8> : das_scatter_kernel<false, 16>);
+  cudaError_t e = ensure_smem(kern, smem);
+  if (e != cudaSuccess) return e;
+  const int64_t gx = (P.n_fast + P.tile_f - 1) / P.tile_f;
+  const int64_t gy = P.slow_tile1 - P.slow_tile0;
+  if (gx <= 0 || gy <= 0) return cudaSuccess;
+  kern<<<dim3((unsigned)gx, (unsigned)gy), nthr, smem, st>>>(P, X, Ya);
+  return cudaGetLastError();
+}
+
+// Column pass after an unweighted scatter S = DAS^T g: dW[c] = sum_k Y[k, c] *
+// S[k, c] (the weight gradient: each term g[n] * Y[k(n,c), c] regrouped by
+// sample), and, when w is given, S[:, c] *= w[c] in place (the weighted
+// adjoint). One CTA per column; columns are K apart in both arrays.
+__global__ void __launch_bounds__(256) column_dot_scale_kernel(const float *__restrict__ Y, float *__restrict__ S,
+                                                               const float *__restrict__ w, float *__restrict__ dW,
+                                                               int64_t K) {
+  const int64_t c = blockIdx.x;
+  const float *y = Y ? Y + c * K : nullptr;
+  float *sc = S + c * K;
+  const float wc = w ? __ldg(w + c) : 1.0f;
+  float acc = 0.0f;
+  for (int64_t k = threadIdx.x; k < K; k += blockDim.x) {
+    const float v = sc[k];
+    if (y) acc = fmaf(__ldg(y + k), v, acc);
+    if (w) sc[k] = v * wc;
+  }
+  if (dW == nullptr) return;
+  __shared__ float red[8];
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
   __syncthreads();
-  if (ADJ) {
-    for (int j = 0; j < jn; j++) {
-      float *dst = Ya + ((int64_t)o * n_in + i0 + j) * K;
-      for (int64_t k = tid; k < K; k += nthr) {
-        const float v = hist[(int64_t)j * K + k];
-        if (splits == 1) dst[k] = v;
-        else if (v != 0.0f) atomicAdd(dst + k, v);
-      }
-    }
-  }
-  if (WG) {
-    const int lane = tid & 31, warp = tid >> 5, nw = nthr >> 5;
-#pragma unroll
-    for (int j = 0; j < CW; j++) {
-      float v = wsum[j];
-      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-      if (lane == 0) red[j * nw + warp] = v;
-    }
-    __syncthreads();
-    if (tid < jn) {
-      float v = wacc[tid];
-      for (int w = 0; w < nw; w++) v += red[tid * nw + w];
-      atomicAdd(dW + (int64_t)o * n_in + i0 + tid, v);
-    }
+  if (threadIdx.x == 0) {
+    float t = 0.0f;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += red[q];
+    dW[c] = t;
   }
 }
 
-}  // namespace
-
-cudaError_t build_leg_tables(const FastParams &P, int64_t *TA, int64_t *TB, int *range, cudaStream_t st) {
-  const int n_out = (P.method == RCA_ROWTX) ? P.Nr : P.Nt;
-  const int n_in = (P.method == RCA_ROWTX) ? P.Nt : P.Nr;
-  const int init[7] = {INT_MAX, INT_MIN, INT_MAX, INT_MIN, 0, 0, 0};
-  cudaError_t e = cudaMemcpyAsync(range, init, sizeof(init), cudaMemcpyHostToDevice, st);
-  if (e != cudaSuccess) return e;
-  if (P.No > 0) {
-    dim3 grid((unsigned)((P.No + 255) / 256), (unsigned)(n_out + n_in));
-    legtab_kernel<<<grid, 256, 0, st>>>(P, TA, TB, range);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+cudaError_t launch_column_dot_scale(const float *Y, float *S, const float *w, float *dW, int64_t K, int64_t ncol,
+                                    cudaStream_t st) {
+  if (ncol <= 0 || (K <= 0 && dW == nullptr)) return cudaSuccess;
+  for (int64_t c0 = 0; c0 < ncol; c0 += 2147483647) {
+    const int64_t n = std::min<int64_t>(ncol - c0, 2147483647);
+    column_dot_scale_kernel<<<(unsigned)n, 256, 0, st>>>(Y ? Y + c0 * K : nullptr, S + c0 * K, w ? w + c0 : nullptr,
+                                                         dW ? dW + c0 : nullptr, K);
   }
-  legtab_classify_kernel<<<1, 1, 0, st>>>(range, P.K, (int64_t)n_out * n_in * P.K);
   return cudaGetLastError();
-}
-
-cudaError_t launch_tab_gather(const FastParams &P, const int64_t *TA, const int64_t *TB, const int *range,
-                              cudaStream_t st) {
-  if (P.No <= 0) return cudaSuccess;
-  const unsigned g = (unsigned)((P.No + 255) / 256);
-  if (P.w) tab_gather_kernel<float, true><<<g, 256, 0, st>>>(P, TA, TB, range);
-  else tab_gather_kernel<float, false><<<g, 256, 0, st>>>(P, TA, TB, range);
-  return cudaGetLastError();
-}
-
-// Columns per CTA of the column-owner kernels: a power of two, at most 16
-// for the adjoint (histograms of width x K x 4 bytes within 50 KB, so four
-// CTAs fit on an SM) and 4 for the weight gradient, no wider than the next
-// power of two >= n_in. Narrow CTAs re-read the outer leg table more often
-// but keep more warps resident, which is what these latency-bound loops need
-// (CG configuration: scatter 0.19 ms at width 4 vs 0.26 ms at width 8).
-int colowner_width(int64_t K, int n_in, bool adj) {
-  int cw = adj ? 16 : 4;
-  while (adj && cw > 1 && (size_t)cw * K * 4 > 50 * 1024) cw >>= 1;
-  while (cw > 1 && cw / 2 >= n_in) cw >>= 1;
-  return cw;
-}
-
-namespace {
-
-template <bool ADJ, bool WG, int CW>
-cudaError_t colowner_launch(const FastParams &P, const int64_t *TA, const int64_t *TB, const float *X, const float *G,
-                            float *Ya, float *dW, dim3 grid, size_t smem, int splits, cudaStream_t st) {
-  constexpr int PX = 1;  // two points per thread: more loads in flight but 104 registers, slower
-  cudaError_t e = ensure_smem(tab_colowner_kernel<ADJ, WG, CW, PX>, smem);
-  if (e != cudaSuccess) return e;
-  tab_colowner_kernel<ADJ, WG, CW, PX><<<grid, 256, smem, st>>>(P, TA, TB, X, G, Ya, dW, splits);
-  return cudaGetLastError();
-}
-
-template <bool ADJ, bool WG>
-cudaError_t colowner_dispatch(int cw, const FastParams &P, const int64_t *TA, const int64_t *TB, const float *X,
-                              const float *G, float *Ya, float *dW, dim3 grid, size_t smem, int splits,
-                              cudaStream_t st) {
-  switch (cw) {
-    case 16: return colowner_launch<ADJ, WG, 16>(P, TA, TB, X, G, Ya, dW, grid, smem, splits, st);
-    case 8: return colowner_launch<ADJ, WG, 8>(P, TA, TB, X, G, Ya, dW, grid, smem, splits, st);
-    case 4: return colowner_launch<ADJ, WG, 4>(P, TA, TB, X, G, Ya, dW, grid, smem, splits, st);
-    case 2: return colowner_launch<ADJ, WG, 2>(P, TA, TB, X, G, Ya, dW, grid, smem, splits, st);
-    default: return colowner_launch<ADJ, WG, 1>(P, TA, TB, X, G, Ya, dW, grid, smem, splits, st);
-  }
-}
-
-}  // namespace
-
-cudaError_t launch_tab_colowner(const FastParams &P, const int64_t *TA, const int64_t *TB, const float *X,
-                                const float *G, float *Ya, float *dW, bool adj, bool wg, int sm_count,
-                                cudaStream_t st) {
-  const int n_out = (P.method == RCA_ROWTX) ? P.Nr : P.Nt;
-  const int n_in = (P.method == RCA_ROWTX) ? P.Nt : P.Nr;
-  if (n_out == 0 || n_in == 0) return cudaSuccess;
-  const int cw = colowner_width(P.K, n_in, adj);
-  const int jmax = std::min(cw, n_in);
-  if (adj && (size_t)jmax * P.K * 4 > 200 * 1024) return cudaErrorInvalidValue;  // A-scans too long for the histogram
-  const int groups = (n_in + cw - 1) / cw;
-  const int64_t ctas = (int64_t)n_out * groups;
-  int splits = (int)std::max<int64_t>(1, std::min<int64_t>(64, (4 * (int64_t)sm_count + ctas - 1) / ctas));
-  if (P.No < 4096) splits = 1;
-  const size_t smem = (adj ? (size_t)jmax * P.K * 4 : 0) + (wg ? (size_t)cw * 8 * 4 + cw * 4 : 0);
-  dim3 grid((unsigned)n_out, (unsigned)groups, (unsigned)splits);
-  if (adj && wg) return colowner_dispatch<true, true>(cw, P, TA, TB, X, G, Ya, dW, grid, smem, splits, st);
-  if (adj) return colowner_dispatch<true, false>(cw, P, TA, TB, X, G, Ya, dW, grid, smem, splits, st);
-  return colowner_dispatch<false, true>(cw, P, TA, TB, X, G, Ya, dW, grid, smem, splits, st);
 }
 
 }  // namespace dream

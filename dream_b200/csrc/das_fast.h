@@ -42,22 +42,17 @@ struct FastParams {
 
 size_t fast_smem_bytes(const FastParams &P, int nthr);
 cudaError_t launch_fast(const FastParams &P, bool bf16, cudaStream_t st);
+// Adjoint on the forward's tiles: Ya[k(n,c), c] += w[c] * X[n] (FP32 A-scans;
+// P.w may be NULL). Adds into Ya, which the caller zeroes first.
+cudaError_t launch_scatter(const FastParams &P, const float *X, float *Ya, cudaStream_t st);
+// Per column c of K x ncol arrays: dW[c] = sum_k Y[k,c] * S[k,c] (when Y and dW
+// are given), then S[:, c] *= w[c] (when w is given).
+cudaError_t launch_column_dot_scale(const float *Y, float *S, const float *w, float *dW, int64_t K, int64_t ncol,
+                                    cudaStream_t st);
 cudaError_t convert_f32_to_bf16(const float *x, void *y, int64_t n, cudaStream_t st);
 // rows x row_elems block of a row-pitched array (same offsets in x and y)
 cudaError_t convert_f32_to_bf16_2d(const float *x, void *y, int64_t rows, int64_t row_elems, int64_t pitch,
                                    cudaStream_t st);
-
-// Geometry-bound operator (leg tables; FP32 samples).
-// range: 7 ints of device scratch written by build_leg_tables.
-cudaError_t build_leg_tables(const FastParams &P, int64_t *TA, int64_t *TB, int *range, cudaStream_t st);
-cudaError_t launch_tab_gather(const FastParams &P, const int64_t *TA, const int64_t *TB, const int *range,
-                              cudaStream_t st);
-// Adjoint scatter (Ya must be zero when splits > 1; the launcher zeroes nothing)
-// and/or weight gradient (dW accumulated atomically: zero it first).
-cudaError_t launch_tab_colowner(const FastParams &P, const int64_t *TA, const int64_t *TB, const float *X,
-                                const float *G, float *Ya, float *dW, bool adj, bool wg, int sm_count,
-                                cudaStream_t st);
-int colowner_width(int64_t K, int n_in, bool adj);
 
 // Persistent batch launch over (frame, tile_f index, tile_s index) items
 // (int4: frame, tfi, tsi, unused); resets the queue counter *ctr first.

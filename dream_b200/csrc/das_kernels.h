@@ -25,7 +25,8 @@ struct PlainLaunch {
   int64_t K;
   const void *Ro;
   int64_t No;
-  int64_t no0, no1;  // pixel range of this launch
+  int64_t no0, no1;  // pixel range of this launch (warp-patch range when n_fast > 0)
+  int64_t n_fast;    // grid hint: points along the grid's fast axis (0: none)
   const void *Gt;
   int64_t Nt;
   const void *Gr;

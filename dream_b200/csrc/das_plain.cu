@@ -9,7 +9,9 @@
 //   RCA row-tx  extra_src/das.cc:533-626, opencl/das_uni_double.cl:283-394
 // Each thread owns one image point and sums its terms in the reference order
 // (outer element loop, inner element loop), so the image is bit-identical to
-// the reference CPU code, not merely close to it.
+// the reference CPU code, not merely close to it. With a grid hint the warps
+// take 8 x 4 patches of the image grid instead of 32 consecutive points, which
+// changes only which thread owns which point.
 //
 // What differs from the reference is where the work goes. The inner-loop
 // element leg (receive leg for TFM/col-tx, column leg for row-tx) depends
@@ -32,7 +34,8 @@ struct PlainParams {
   int Nt;
   const T *Gr;
   int Nr;
-  int64_t no0, no1;  // pixel range [no0, no1) of this launch
+  int64_t no0, no1;  // pixel range [no0, no1) of this launch, or warp-patch range when n_fast > 0
+  int64_t n_fast, n_slow;  // grid hint: warps take 8 x 4 patches of (fast, slow) points
   const T *delay;  // das: device delays in us (1 value, or No when delay_multi)
   int delay_multi;
   T delay_ms;      // das_uni: the scalar delay in ms
@@ -92,9 +95,24 @@ __global__ void __launch_bounds__(256) das_plain_kernel(const PlainParams<T> P) 
   T *tab = reinterpret_cast<T *>(smem_raw);
   const int tid = threadIdx.x;
   const int bd = blockDim.x;
-  const int64_t no_raw = P.no0 + (int64_t)blockIdx.x * bd + tid;
-  const bool active = no_raw < P.no1;
-  const int64_t no = active ? no_raw : P.no0;
+  const int64_t gt = (int64_t)blockIdx.x * bd + tid;
+  int64_t no_raw;
+  bool active;
+  if (P.n_fast > 0) {
+    // 2-D patches: a warp covers 8 points along the grid's fast axis x 4 along
+    // the slow one, so its 32 gathers of one A-scan column fall on a few lines
+    const int64_t wp = P.no0 + (gt >> 5);
+    const int lane = tid & 31;
+    const int64_t nwf = (P.n_fast + 7) >> 3;
+    const int64_t pf = wp % nwf, ps = wp / nwf;
+    const int64_t f = pf * 8 + (lane & 7), s = ps * 4 + (lane >> 3);
+    active = wp < P.no1 && f < P.n_fast && s < P.n_slow;
+    no_raw = s * P.n_fast + f;
+  } else {
+    no_raw = P.no0 + gt;
+    active = no_raw < P.no1;
+  }
+  const int64_t no = active ? no_raw : 0;  // inactive lanes read point 0 and write nothing
 
   // ---- image point ----
   T xo, yo, zo;
@@ -288,7 +306,8 @@ static cudaError_t launch_one(const PlainParams<T> &P, int bd, size_t smem, cuda
                                          : das_plain_kernel<T, M, UNI, TAB, false, IDX>;
   cudaError_t e = ensure_smem(kern, smem);
   if (e != cudaSuccess) return e;
-  int64_t grid = (P.no1 - P.no0 + bd - 1) / bd;
+  const int64_t threads = (P.no1 - P.no0) * (P.n_fast > 0 ? 32 : 1);  // patches of 32 points, or points
+  int64_t grid = (threads + bd - 1) / bd;
   kern<<<(unsigned)grid, bd, smem, st>>>(P);
   return cudaGetLastError();
 }
@@ -327,6 +346,8 @@ static PlainParams<T> make_params(const PlainLaunch &L) {
   P.No = L.No;
   P.no0 = L.no0;
   P.no1 = L.no1;
+  P.n_fast = L.n_fast;
+  P.n_slow = L.n_fast > 0 ? L.No / L.n_fast : 0;
   P.Gt = (const T *)L.Gt;
   P.Nt = (int)L.Nt;
   P.Gr = (const T *)L.Gr;

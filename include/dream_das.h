@@ -228,6 +228,20 @@ int dream_das_get_tile(const dream_das_plan *plan, int *tile_f, int *tile_s);
 int dream_das_set_chunk(dream_das_plan *plan, int jc);
 
 /*
+ * Inner-element shard of an F32_STORE / BF16_STORE plan (TFM and RCA; no
+ * counterpart in the reference). After dream_das_set_inner_shard(plan, lo, hi)
+ * the A-scans passed to the device entry points hold only the columns of
+ * inner elements [lo, hi) (TFM: receivers; RCA col-tx: rows; RCA row-tx:
+ * columns), column (o, i) at o * (hi - lo) + (i - lo), and the image is the
+ * partial sum over those terms; Gt and Gr stay the full element arrays (the
+ * RCA stripe edges are read from them). Ranks that each hold one shard of an
+ * RCA frame add their partial images (one all-reduce) to get the frame.
+ * lo = hi = 0 restores the full layout. The host entry dream_das_run refuses a
+ * sharded plan.
+ */
+int dream_das_set_inner_shard(dream_das_plan *plan, int64_t lo, int64_t hi);
+
+/*
  * L2 blocking of the F32_STORE / BF16_STORE kernels (TFM, RCA; no counterpart
  * in the reference, whose CPU loops have no such cache to fit). A-scans larger
  * than the budget are beamformed in passes over ranges of inner elements (a
@@ -257,16 +271,20 @@ int dream_das_weighted_run_device(dream_das_plan *plan, const void *dY, const vo
  * adjoint; its explicit DAS matrix example (examples/model_based_example.m:
  * 381-456) is what this replaces.
  *
- * dream_das_bind_geometry computes the FP64 leg tables once (plan-owned
- * device memory, (Nt+Nr)*No*8 bytes) and keeps the device pointers dRo, dGt,
- * dGr, ddelay, which must stay valid while bound. With the A-scan column
- * index c and the FP64 reference sample index k(n, c):
+ * dream_das_bind_geometry keeps the device pointers dRo, dGt, dGr, ddelay
+ * (which must stay valid while bound) and the constants; nothing is
+ * precomputed: every operator forms its legs per image tile, as the FP32/BF16
+ * storage kernels do. With the A-scan column index c and the FP64 reference
+ * sample index k(n, c):
  *   forward  Im[n]    = sum_c w[c] * Y[k(n,c), c]          (w NULL: all ones)
  *   adjoint  Ya[k, c] = w[c] * sum_{n: k(n,c)=k} X[n]       (Ya overwritten)
  *   wgrad    dW[c]    = sum_n G[n] * Y[k(n,c), c]           (dW overwritten)
- *   backward adjoint(G, w) into dYg and wgrad(G, Y) into dWg in one pass
- * All are asynchronous on `stream`; forward adds out-of-bounds terms to
- * d_oob when it is not NULL.
+ *   backward adjoint(G, w) into dYg and wgrad(G, Y) into dWg
+ * wgrad is computed as sum_k Y[k,c] * (adjoint of G, unweighted)[k,c] through
+ * a plan-owned scratch of K x columns floats; backward uses dYg for it. All
+ * are asynchronous on `stream`; forward adds out-of-bounds terms to d_oob
+ * when it is not NULL. The image tiling follows dream_das_set_grid_hint /
+ * dream_das_set_tile / dream_das_set_chunk.
  */
 int dream_das_bind_geometry(dream_das_plan *plan, const void *dRo, const void *dGt, const void *dGr,
                             double dt, int delay_type, const void *ddelay, double cp, void *stream);

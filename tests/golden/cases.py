@@ -122,3 +122,11 @@ for prec in ("f64", "f32"):
     CASES[f"near_element_{prec}"] = dict(kind="near_element", kw=dict(delay=-0.03), prec=prec, err="ignore")
     CASES[f"near_element_oob_{prec}"] = dict(kind="near_element", kw=dict(delay=-0.045), prec=prec,
                                              err="warn")
+
+
+RCA_SLABS = (0, 101, 255)  # z-planes of the RCA configuration's 128 x 128 x 256 grid (z is the fastest index)
+
+
+def rca_slab_points(nz=256, n_xy=128 * 128, slabs=RCA_SLABS):
+    """Indices of every (x, y) point of the given z-planes of synth.grid_xyz."""
+    return np.sort(np.concatenate([iz + nz * np.arange(n_xy) for iz in slabs]))

@@ -11,6 +11,11 @@ pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
 
+def das_scatter(x, w, op):
+    from dream_b200.autograd import das_scatter as f
+    return f(x, w, op)
+
+
 @pytest.fixture(scope="module", autouse=True)
 def _cuda():
     if not torch.cuda.is_available():
@@ -76,25 +81,36 @@ def test_dot_product_full_cg_config():
 
 
 def _loss(op, x, w, Y, lam):
-    from dream_b200.autograd import das_scatter
     R = das_scatter(x, w, op)
     return ((R.double() - Y.double()) ** 2).sum() + lam * (x.double() ** 2).sum()
 
 
-def test_gradients_fd_and_cpu_reference():
+GRAD_CONFIGS = {
+    # a reduced problem: 8 x 8 elements, 32 x 32 image
+    "reduced_8x8_32x32": dict(seed=6, n_el=8, K=1024, nx=32, nz=32, density=0.05, x_rng=(-4.0, 4.0),
+                              z_rng=(5.0, 15.0)),
+    # the model-based reconstruction configuration: 32 x 32 elements, K = 2048, 256 x 256 image
+    "cg_32x32_K2048_256x256": dict(seed=4),
+}
+
+
+@pytest.mark.parametrize("cfg", sorted(GRAD_CONFIGS))
+def test_gradients_fd_and_cpu_reference(cfg):
     """Gradients of ||DAS_w^T x - Y||^2 + lam||x||^2 w.r.t. x and w: autograd vs
-    central finite differences (h = 1e-3) and vs the FP64 CPU reference."""
+    central finite differences (h = 1e-3) on 6 weights and 6 image points, and
+    vs the FP64 CPU reference on the oracle's index table."""
     from dream_b200 import synth
     from dream_b200.autograd import DASOperator
-    s = synth.cg_scene(seed=6, n_el=8, K=1024, nx=32, nz=32, density=0.05, x_rng=(-4.0, 4.0), z_rng=(5.0, 15.0))
-    op = DASOperator(s.Gt, s.Gr, s.Ro, s.dt, s.delay, s.cp, "tfm", 1024)
-    _, _, _, idx = oracle.das(np.zeros((1024, 64)), s.Gt, s.Gr, s.Ro, s.dt, s.delay, s.cp, "tfm", "ignore",
+    s = synth.cg_scene(**GRAD_CONFIGS[cfg])
+    K = s.Y.shape[0]
+    op = DASOperator(s.Gt, s.Gr, s.Ro, s.dt, s.delay, s.cp, "tfm", K)
+    _, _, _, idx = oracle.das(np.zeros((K, op.ncol)), s.Gt, s.Gr, s.Ro, s.dt, s.delay, s.cp, "tfm", "ignore",
                               np.float64, return_idx=True)
     lam = 1e-3
     rng = np.random.default_rng(2)
     x0 = f32(s.extra["reflectivity"] + 0.1 * rng.normal(size=op.No))
     w0 = f32(rng.uniform(0.5, 1.5, op.ncol))
-    Ytrue = oracle.adjoint(idx, s.extra["reflectivity"], np.ones(op.ncol), 1024)
+    Ytrue = oracle.adjoint(idx, s.extra["reflectivity"], np.ones(op.ncol), K)
     Ynp = f32(Ytrue + 0.01 * rng.normal(size=Ytrue.shape))
     Y = torch.from_numpy(np.ascontiguousarray(Ynp.T)).float().cuda().t()
     x = torch.from_numpy(x0).float().cuda().requires_grad_(True)
@@ -103,23 +119,38 @@ def test_gradients_fd_and_cpu_reference():
     gx, gw = torch.autograd.grad(L, (x, w))
     gx, gw = gx.double().cpu().numpy(), gw.double().cpu().numpy()
     # CPU reference (FP64 on the oracle index table)
-    R = oracle.adjoint(idx, x0, w0, 1024) - Ynp
+    R = oracle.adjoint(idx, x0, w0, K) - Ynp
     ref_gx = 2.0 * oracle.weighted(idx, R, w0) + 2.0 * lam * x0
     ref_gw = 2.0 * oracle.wgrad(idx, x0, R)
     assert np.abs(gx - ref_gx).max() <= 1e-4 * np.abs(ref_gx).max()
     assert np.abs(gw - ref_gw).max() <= 1e-4 * np.abs(ref_gw).max()
-    # central finite differences, h = 1e-3
+    # Central finite differences, h = 1e-3. Perturbing w[c] changes only column c
+    # of DAS_w^T x, and x[n] only the samples k(n, c'); every other term of the
+    # loss is equal in exact arithmetic at w +- e and x +- e, so each difference
+    # is summed over the touched entries (plus the regulariser): the same
+    # derivative, without the FP32 rounding of the untouched entries, which
+    # depends on the order of the scatter's additions and would swamp the
+    # 2*h*grad difference on the full configuration.
     h = 1e-3
+    Yd = Y.double()
     with torch.no_grad():
         for c in rng.choice(op.ncol, 6, replace=False):
             e = torch.zeros_like(w)
             e[c] = h
-            fd = float(_loss(op, x, w + e, Y, lam) - _loss(op, x, w - e, Y, lam)) / (2 * h)
+            Lc = lambda ww: float(((das_scatter(x, ww, op)[:, c].double() - Yd[:, c]) ** 2).sum())
+            fd = (Lc(w + e) - Lc(w - e)) / (2 * h)
             assert abs(fd - gw[c]) <= 2e-3 * max(abs(gw[c]), 1e-3 * np.abs(gw).max())
         for n in rng.choice(op.No, 6, replace=False):
             e = torch.zeros_like(x)
             e[n] = h
-            fd = float(_loss(op, x + e, w, Y, lam) - _loss(op, x - e, w, Y, lam)) / (2 * h)
+            cols = np.nonzero(idx[:, n] != oracle.OOB_MISS)[0]
+            ks = torch.from_numpy(idx[cols, n]).cuda()
+            cs = torch.from_numpy(cols).cuda()
+
+            def Ln(xx):
+                R = das_scatter(xx, w, op)[ks, cs].double() - Yd[ks, cs]
+                return float((R ** 2).sum()) + lam * float((xx.double()[n]) ** 2)
+            fd = (Ln(x + e) - Ln(x - e)) / (2 * h)
             assert abs(fd - gx[n]) <= 2e-3 * max(abs(gx[n]), 1e-3 * np.abs(gx).max())
 
 

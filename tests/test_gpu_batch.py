@@ -1,5 +1,6 @@
 """Batched DAS: one persistent launch over uneven frames (and its CUDA graph)
-equals the per-frame FP32-storage kernel; the autotuner's choices are valid."""
+against the reference's FP64 image of the same stored samples, and the
+per-frame FP32-storage kernel; the autotuner's choices are valid."""
 import numpy as np
 import pytest
 
@@ -27,26 +28,43 @@ def _frames(n=6, seed=11, max_side=160, storage="f32"):
     return frames
 
 
+def _expected(f, storage):
+    """The frame's image from the reference das (oracle/_ref; the C oracle when
+    absent) on exactly the stored samples (FP32 or BF16 values in FP64), so
+    every sum is exact and every index is the reference's FP64 index."""
+    from oracle import oracle
+    Ys = np.asfortranarray(f.Y.float().t().contiguous().t().cpu().numpy().astype(np.float64))
+    args = [np.asfortranarray(a.cpu().numpy()) for a in (f.Gt, f.Gr, f.Ro, f.delay)]
+    mod = oracle.reference_module("f64")
+    if mod is not None:
+        return mod.das(Ys, args[0], args[1], args[2], f.dt, args[3], f.cp, f.method, "ignore", "cpu", "")
+    return oracle.das(Ys, args[0], args[1], args[2], f.dt, args[3], f.cp, f.method, "ignore", np.float64)[0]
+
+
 def _single(f, storage):
-    """The one-frame kernel on the same stored samples (its own tile; the
-    per-pixel summation order only depends on the inner-chunk length)."""
+    """The one-frame kernel on the same stored samples."""
     from dream_b200.beamformer import das_mixed
     Y = f.Y.float() if storage == "bf16" else f.Y
     return das_mixed(Y, f.Gt, f.Gr, f.Ro, f.dt, f.delay, f.cp, "tfm", "ignore", "cuda", storage)
 
 
 @pytest.mark.parametrize("storage", ["f32", "bf16"])
-def test_batch_matches_single_frames(storage):
+def test_batch_matches_oracle(storage):
+    """Every frame of one persistent launch against the reference's FP64 image
+    of the same stored samples (1e-6 of max|Im|: a wrong index moves a pixel by
+    O(1)), and against the one-frame kernel."""
     from dream_b200.batch import DASBatch
     frames = _frames(storage=storage)
     b = DASBatch(frames, storage=storage)
     assert b.items > 0 and b.grid > 0
     b.run()
     torch.cuda.synchronize()
-    for f in frames:
-        ref = _single(f, storage)
-        scale = float(ref.abs().max())
-        assert float((f.Im - ref).abs().max()) <= 1e-6 * scale
+    for i, f in enumerate(frames):
+        ref = _expected(f, storage)
+        got = f.Im.cpu().numpy().astype(np.float64)
+        scale = np.abs(ref).max()
+        assert np.abs(got - ref).max() <= 1e-6 * scale, f"frame {i}"
+        assert float((f.Im - _single(f, storage)).abs().max()) <= 1e-6 * scale, f"frame {i}"
 
 
 def test_batch_graph_replay_and_new_data():
@@ -60,7 +78,8 @@ def test_batch_graph_replay_and_new_data():
     torch.cuda.synchronize()
     first = [f.Im.clone() for f in frames]
     for f, r in zip(frames, first):
-        assert float((r - _single(f, "f32")).abs().max()) <= 1e-6 * float(r.abs().max())
+        ref = _expected(f, "f32")
+        assert np.abs(r.cpu().numpy().astype(np.float64) - ref).max() <= 1e-6 * np.abs(ref).max()
     # new A-scans in the same buffers: the replay reads them
     for f in frames:
         f.Y.mul_(-2.0)

@@ -8,7 +8,7 @@ reference's exactly (np.array_equal), not merely within 1e-12 / 1e-5.
 import numpy as np
 import pytest
 
-from cases import CASES, build_scene
+from cases import rca_slab_points, CASES, build_scene
 from gen_golden import UNI_CASES, materialise_uni, uni_Y
 from oracle import oracle
 
@@ -129,30 +129,32 @@ def test_saft_full_config(prec):
 
 
 @pytest.mark.parametrize("prec", ["f64", "f32"])
-def test_tfm_full_config_pixel_subset(prec):
-    """Full TFM configuration (64x64 FMC, K=3000, 512x512): the whole image on
-    the GPU, 4096 seeded pixels checked against the reference/oracle."""
+def test_tfm_full_config_whole_image(prec):
+    """Full TFM configuration (64x64 FMC, K=3000, 512x512): all 262,144 pixels
+    of the GPU image equal the reference das / das_f (oracle/_ref, the
+    reference's own code; the C oracle when absent) bit for bit."""
     from dream_b200 import synth
     dtype = np.float64 if prec == "f64" else np.float32
     s = synth.tfm_scene(seed=1).astype(dtype)
     Im = _run(prec, s, "stop", "device")
-    sel = np.sort(np.random.default_rng(7).choice(s.Ro.shape[0], 4096, replace=False))
-    sub = s.astype(dtype)
-    sub.Ro = np.asfortranarray(s.Ro[sel])
-    assert np.array_equal(Im[sel], _expected(prec, sub, "stop"))
+    ref = _expected(prec, s, "stop")
+    assert Im.shape == ref.shape == (512 * 512,)
+    assert np.array_equal(Im, ref), f"{np.sum(Im != ref)} pixels differ"
 
 
 @pytest.mark.parametrize("method", ["rca_rowtx", "rca_coltx"])
-def test_rca_full_config_pixel_subset(method):
+def test_rca_full_config_z_slabs(method):
     """Full RCA configuration (128x128 row-column array, K=4096, 128x128x256
-    grid) in FP32: whole image on the GPU, 1024 seeded pixels vs the oracle."""
+    grid) in FP32: the whole image on the GPU; three whole 128x128 z-planes
+    (49,152 pixels) equal the reference das_f bit for bit."""
     from dream_b200 import synth
     s = synth.rca_scene(seed=2, method=method).astype(np.float32)
     Im = _run("f32", s, "stop", "device")
-    sel = np.sort(np.random.default_rng(8).choice(s.Ro.shape[0], 1024, replace=False))
+    sel = rca_slab_points()
     sub = s.astype(np.float32)
     sub.Ro = np.asfortranarray(s.Ro[sel])
-    assert np.array_equal(Im[sel], _expected("f32", sub, "stop"))
+    ref = _expected("f32", sub, "stop")
+    assert np.array_equal(Im[sel], ref), f"{np.sum(Im[sel] != ref)} pixels differ"
 
 
 def test_empty_and_degenerate_inputs():
