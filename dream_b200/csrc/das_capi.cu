@@ -250,22 +250,28 @@ unsigned long long *bad_counter(dream_das_plan *p) {
 int launch_plain(dream_das_plan *p, PlainLaunch &L, cudaStream_t st) {
   L.ny = p->K * num_columns(p);
   L.bad = bad_counter(p);
-  // 2-D warp patches when the plan has a grid hint (das_uni: its own grid)
+  // 2-D warp patches for RCA volumes with a grid hint (das_uni: its own
+  // grid). On the 128x128-element RCA volume (128x128x256 points) they take
+  // plain FP32 from 194.8 to 180.7 ms; on the 64x64-element TFM frame
+  // (512x512 points) they cost 4 % (FP64 2.43 -> 2.52 ms), so TFM and SAFT
+  // keep warps of consecutive points.
   L.n_fast = 0;
-  if (L.uni) {
-    const int64_t nf = L.Ny > 1 ? L.Ny : L.Ny * L.Nz;
-    if (nf >= 8 && L.No % nf == 0 && nf < L.No) L.n_fast = nf;
-  } else if (p->n_fast >= 8 && p->n_fast < L.No) {
-    L.n_fast = p->n_fast;
+  if (L.method == DREAM_DAS_RCA_COLTX || L.method == DREAM_DAS_RCA_ROWTX) {
+    if (L.uni) {
+      const int64_t nf = L.Ny > 1 ? L.Ny : L.Ny * L.Nz;
+      if (nf >= 8 && L.No % nf == 0 && nf < L.No) L.n_fast = nf;
+    } else if (p->n_fast >= 8 && p->n_fast < L.No) {
+      L.n_fast = p->n_fast;
+    }
   }
   // Pixel chunks keep a cancellation request observable between launches.
   const int64_t tpp = std::max<int64_t>(terms_per_pixel(p), 1);
   int64_t chunk = std::max<int64_t>(int64_t(1) << 16, (int64_t(1) << 33) / tpp);
   chunk = (chunk + 255) / 256 * 256;
   int64_t total = L.No;
-  if (L.n_fast > 0) {  // the range is over 8 x 4 warp patches
-    total = ((L.n_fast + 7) / 8) * ((L.No / L.n_fast + 3) / 4);
-    chunk = std::max<int64_t>(8, chunk / 32);
+  if (L.n_fast > 0) {  // the range is over rows of warp patches (at most 65535 per launch: the grid's y extent)
+    total = (L.No / L.n_fast + PLAIN_PATCH_S - 1) / PLAIN_PATCH_S;
+    chunk = std::min<int64_t>(65535, std::max<int64_t>(1, chunk / (PLAIN_PATCH_S * L.n_fast)));
   }
   for (int64_t s = 0; s < total; s += chunk) {
     if (p->cancelled.load()) return fail(DREAM_ERR_CANCELLED, "DAS cancelled");
@@ -471,15 +477,17 @@ int launch_fast_plan(dream_das_plan *p, const void *dY, const void *dRo, const v
   if (!apply_shard(p, F)) return 0;  // Y holds the columns of inner elements [shard_lo, shard_hi) only
   const int64_t col_bytes = (int64_t)n_out * p->K * (bf16 ? 2 : 4);  // A-scans of one inner element
   const int64_t y_bytes = col_bytes * n_in;
-  // automatic: passes of at most 96 MB once the A-scans exceed 160 MB (RCA
-  // 128x128, K 4096, FP32: 268 MB in 3 passes, 54.7 -> 45.8 ms; smaller passes
-  // lose more to the per-pass leg set-up than they gain in L2 hits, and the
-  // 134 MB BF16 frame is as fast unsplit)
+  // automatic: once the A-scans exceed 112 MB (most of the 126 MB L2), even
+  // passes of at most 96 MB, widths multiples of the 16-term register chunk
+  // (RCA 128x128, K 4096: FP32 268 MB in passes of 48/48/32 columns, 51.6 ->
+  // 40.0 ms; BF16 134 MB in two of 64, 36.7 -> 34.5 ms; smaller passes lose
+  // more to the per-pass leg set-up than they gain in L2 hits)
   const int64_t budget = p->l2_block > 0 ? p->l2_block : (int64_t(96) << 20);
-  const int64_t split_above = p->l2_block > 0 ? budget : (int64_t(160) << 20);
+  const int64_t split_above = p->l2_block > 0 ? budget : (int64_t(112) << 20);
   int pass_w = n_in;
   if (in_hi == 0 && p->l2_block >= 0 && y_bytes > split_above) {
-    pass_w = (int)std::max<int64_t>(16, budget / std::max<int64_t>(col_bytes, 1) / 16 * 16);
+    const int64_t n_pass = (y_bytes + budget - 1) / budget;
+    pass_w = (int)std::max<int64_t>(16, ((n_in + n_pass - 1) / n_pass + 15) / 16 * 16);
     pass_w = std::min(pass_w, n_in);
   }
   const int lo0 = F.in_lo, hi0 = F.in_hi > 0 ? F.in_hi : n_in;

@@ -173,11 +173,19 @@ __device__ __noinline__ bool exact_index(const FastParams &P, const Pixel &px, i
   return false;
 }
 
-// Bytes of the tile's shared arrays (TileShared): the host's fast_smem_bytes.
+// Layout of the tile's shared arrays (TileShared): per-element bases,
+// extents and column words first, then (from a 16-byte boundary) the outer
+// legs and the staged inner legs of every thread. The set-up's reduction
+// scratch lives at the start of the outer-leg table until the legs are
+// written. The total is a multiple of 16, so the scatter's windows that follow
+// can be read as int4; for 128 outer and 128 inner elements on a 128-point
+// tile it is 76288 bytes, three blocks per SM.
+__host__ __device__ __forceinline__ size_t tile_head_bytes(int n_out, int n_in) {
+  return ((size_t)(2 * (n_out + n_in) + n_out) * sizeof(int) + 15) & ~(size_t)15;
+}
 __host__ __device__ __forceinline__ size_t fast_smem_bytes_dev(const FastParams &P, int n_out, int n_in, int nthr) {
-  (void)P;
-  return 64 * sizeof(double) + 64 * sizeof(int) + (size_t)(2 * (n_out + n_in) + n_out) * sizeof(int) +
-         (size_t)(n_out + 16) * nthr * sizeof(uint32_t);
+  const size_t legs = (size_t)(n_out + (P.jc == 8 ? 8 : 16)) * nthr * sizeof(uint32_t);
+  return tile_head_bytes(n_out, n_in) + ((legs + 15) & ~(size_t)15);
 }
 
 // A-scan column of term (outer o, inner i): o * n_in + i for a full Y. A Y
@@ -273,8 +281,8 @@ __device__ __forceinline__ void leg_range(const FastParams &P, const TileBox &B,
 }
 
 struct TileShared {
-  double *red;     // [8 warps][8]: box reduction
-  int *stat;       // [8 warps][8]: classification reduction
+  double *red;     // [warps][8]: box reduction (set-up only; shares arel's space)
+  int *stat;       // [warps][8]: classification reduction (set-up only; shares arel's space)
   int *base;       // [n_out + n_in]: integer base of each leg over the tile (outer first)
   int *ext;        // [n_out + n_in]: bound of (floor(leg) - base)
   uint32_t *ahi;   // [n_out]: high word of the outer legs (column offset + base)
@@ -411,10 +419,10 @@ __device__ __forceinline__ void tile_loop(const FastParams &P, const Pixel &px, 
   const int64_t K = P.K;
   for (int i0 = i_lo; i0 < i_hi; i0 += JC) {
     const int jn = min(JC, i_hi - i0);
-    // the chunk's inner legs, one at a time into this thread's shared slots
-    // (computing them side by side in registers would crowd the gather loop)
+    // the chunk's inner legs into this thread's shared slots, four at a time
+    // (all of them side by side in registers would crowd the gather loop)
     bool bad = false;
-#pragma unroll 1
+#pragma unroll 4
     for (int j = 0; j < jn; j++) {
       const int i = i0 + j;
       double dx, dy, dz;
@@ -485,13 +493,14 @@ __device__ __forceinline__ void tile_setup(const FastParams &P, int64_t tfi, int
   const int i_lo = P.in_lo, i_hi = P.in_hi > 0 ? P.in_hi : n_in;
 
   TileShared S;
-  S.red = reinterpret_cast<double *>(smem_raw);
-  S.stat = reinterpret_cast<int *>(S.red + 64);
-  S.base = S.stat + 64;
+  S.base = reinterpret_cast<int *>(smem_raw);
   S.ext = S.base + n_out + n_in;
   S.ahi = reinterpret_cast<uint32_t *>(S.ext + n_out + n_in);
-  S.arel = S.ahi + n_out;
+  S.arel = reinterpret_cast<uint32_t *>(smem_raw + tile_head_bytes(n_out, n_in));
   S.brel = S.arel + n_out * nthr;
+  // n_out * nthr words hold the nwarps * 8 doubles and ints of the set-up
+  S.red = reinterpret_cast<double *>(S.arel);
+  S.stat = reinterpret_cast<int *>(S.red + nwarps * 8);
 
   // ---- image point of this thread (inactive lanes repeat the tile's first point) ----
   const int lf = lane % P.wf, ls = lane / P.wf;
@@ -593,6 +602,7 @@ __device__ __forceinline__ void tile_setup(const FastParams &P, int64_t tfi, int
     hiB = max(hiB, S.stat[w * 8 + 5]);
     extA = max(extA, S.stat[w * 8 + 6]);
   }
+  __syncthreads();  // the scratch is read: the outer legs below may overwrite it
   const int64_t stride = P.ycol_o > 0 ? P.ycol_o : n_in;
   bool exact_tile = bad || ext_max > WIDE_EXTENT || loA > hiA ||
                     (int64_t)n_out * stride * P.K + (int64_t)hiA + hiB + 8448 >= (int64_t(1) << 32) ||
@@ -697,7 +707,7 @@ __global__ void __launch_bounds__(256, 2) das_fast_kernel(const FastParams P) {
 // descriptor is staged in shared memory; every frame's tile has blockDim.x
 // points. ctr must be zero at launch (the batch run resets it).
 template <class YT>
-__global__ void __launch_bounds__(128, 4) das_batch_kernel(const FastParams *__restrict__ frames,
+__global__ void __launch_bounds__(128, 3) das_batch_kernel(const FastParams *__restrict__ frames,
                                                         const int4 *__restrict__ items, int n_items,
                                                         int *__restrict__ ctr) {
   extern __shared__ __align__(16) unsigned char smem_raw[];

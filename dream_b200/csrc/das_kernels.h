@@ -18,6 +18,11 @@ struct Consts32 {
   float Fs, ocp, delay_ms;
 };
 
+// Warp patch of the plain kernels under a grid hint: PLAIN_PATCH_F points
+// along the grid's fast axis x (32 / PLAIN_PATCH_F) along the slow one.
+constexpr int PLAIN_PATCH_F = 8;
+constexpr int PLAIN_PATCH_S = 32 / PLAIN_PATCH_F;
+
 struct PlainLaunch {
   int method;  // 0 SAFT, 1 TFM, 2 RCA col-tx, 3 RCA row-tx
   bool uni;
@@ -25,7 +30,7 @@ struct PlainLaunch {
   int64_t K;
   const void *Ro;
   int64_t No;
-  int64_t no0, no1;  // pixel range of this launch (warp-patch range when n_fast > 0)
+  int64_t no0, no1;  // pixel range of this launch (patch-row range when n_fast > 0)
   int64_t n_fast;    // grid hint: points along the grid's fast axis (0: none)
   const void *Gt;
   int64_t Nt;

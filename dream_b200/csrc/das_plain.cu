@@ -10,8 +10,8 @@
 // Each thread owns one image point and sums its terms in the reference order
 // (outer element loop, inner element loop), so the image is bit-identical to
 // the reference CPU code, not merely close to it. With a grid hint the warps
-// take 8 x 4 patches of the image grid instead of 32 consecutive points, which
-// changes only which thread owns which point.
+// take 8 x 4 patches of the image grid (PLAIN_PATCH_F x PLAIN_PATCH_S) instead
+// of 32 consecutive points, which changes only which thread owns which point.
 //
 // What differs from the reference is where the work goes. The inner-loop
 // element leg (receive leg for TFM/col-tx, column leg for row-tx) depends
@@ -34,8 +34,8 @@ struct PlainParams {
   int Nt;
   const T *Gr;
   int Nr;
-  int64_t no0, no1;  // pixel range [no0, no1) of this launch, or warp-patch range when n_fast > 0
-  int64_t n_fast, n_slow;  // grid hint: warps take 8 x 4 patches of (fast, slow) points
+  int64_t no0, no1;  // pixel range [no0, no1) of this launch, or patch-row range when n_fast > 0
+  int64_t n_fast, n_slow;  // grid hint: warps take patches of (fast, slow) points
   const T *delay;  // das: device delays in us (1 value, or No when delay_multi)
   int delay_multi;
   T delay_ms;      // das_uni: the scalar delay in ms
@@ -88,31 +88,31 @@ __device__ __forceinline__ T load_y(const PlainParams<T> &P, const T *ycol, int6
 
 // IDX: instead of gathering and summing, write every term's sample index
 // (the one the gather would read; -1 for an out-of-bounds term) to P.idx.
-template <class T, int M, bool UNI, bool TAB, bool BIGK, bool IDX = false>
+// PATCH: warps take 2-D patches of the grid (P.n_fast > 0); a template
+// parameter, so the consecutive-point kernel compiles as if it did not exist.
+template <class T, int M, bool UNI, bool TAB, bool BIGK, bool IDX = false, bool PATCH = false>
 __global__ void __launch_bounds__(256) das_plain_kernel(const PlainParams<T> P) {
   using A = Ar<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *tab = reinterpret_cast<T *>(smem_raw);
   const int tid = threadIdx.x;
   const int bd = blockDim.x;
-  const int64_t gt = (int64_t)blockIdx.x * bd + tid;
   int64_t no_raw;
   bool active;
-  if (P.n_fast > 0) {
-    // 2-D patches: a warp covers 8 points along the grid's fast axis x 4 along
-    // the slow one, so its 32 gathers of one A-scan column fall on a few lines
-    const int64_t wp = P.no0 + (gt >> 5);
+  if constexpr (PATCH) {
+    // 2-D patches: warp w of block (x, y) covers PLAIN_PATCH_F points along
+    // the grid's fast axis (patch x * warps + w) x PLAIN_PATCH_S along the
+    // slow one (patch row no0 + y)
     const int lane = tid & 31;
-    const int64_t nwf = (P.n_fast + 7) >> 3;
-    const int64_t pf = wp % nwf, ps = wp / nwf;
-    const int64_t f = pf * 8 + (lane & 7), s = ps * 4 + (lane >> 3);
-    active = wp < P.no1 && f < P.n_fast && s < P.n_slow;
+    const int64_t f = ((int64_t)blockIdx.x * (bd >> 5) + (tid >> 5)) * PLAIN_PATCH_F + lane % PLAIN_PATCH_F;
+    const int64_t s = (P.no0 + blockIdx.y) * PLAIN_PATCH_S + lane / PLAIN_PATCH_F;
+    active = f < P.n_fast && s < P.n_slow;
     no_raw = s * P.n_fast + f;
   } else {
-    no_raw = P.no0 + gt;
+    no_raw = P.no0 + (int64_t)blockIdx.x * bd + tid;
     active = no_raw < P.no1;
   }
-  const int64_t no = active ? no_raw : 0;  // inactive lanes read point 0 and write nothing
+  const int64_t no = active ? no_raw : (PATCH ? 0 : P.no0);  // inactive lanes read a valid point and write nothing
 
   // ---- image point ----
   T xo, yo, zo;
@@ -302,13 +302,21 @@ __global__ void __launch_bounds__(256) das_plain_kernel(const PlainParams<T> P) 
 
 template <class T, int M, bool UNI, bool TAB, bool IDX = false>
 static cudaError_t launch_one(const PlainParams<T> &P, int bd, size_t smem, cudaStream_t st) {
-  auto kern = (sizeof(T) == 4 && P.bigk) ? das_plain_kernel<T, M, UNI, TAB, true, IDX>
-                                         : das_plain_kernel<T, M, UNI, TAB, false, IDX>;
+  const bool patch = P.n_fast > 0, bigk = sizeof(T) == 4 && P.bigk;
+  auto kern = patch ? (bigk ? das_plain_kernel<T, M, UNI, TAB, true, IDX, true>
+                            : das_plain_kernel<T, M, UNI, TAB, false, IDX, true>)
+                    : (bigk ? das_plain_kernel<T, M, UNI, TAB, true, IDX, false>
+                            : das_plain_kernel<T, M, UNI, TAB, false, IDX, false>);
   cudaError_t e = ensure_smem(kern, smem);
   if (e != cudaSuccess) return e;
-  const int64_t threads = (P.no1 - P.no0) * (P.n_fast > 0 ? 32 : 1);  // patches of 32 points, or points
-  int64_t grid = (threads + bd - 1) / bd;
-  kern<<<(unsigned)grid, bd, smem, st>>>(P);
+  dim3 grid;
+  if (patch) {  // [no0, no1) are patch rows; a block holds bd / 32 patches of a row
+    const int64_t wpb = bd >> 5;
+    grid = dim3((unsigned)(((P.n_fast + PLAIN_PATCH_F - 1) / PLAIN_PATCH_F + wpb - 1) / wpb), (unsigned)(P.no1 - P.no0));
+  } else {
+    grid = dim3((unsigned)((P.no1 - P.no0 + bd - 1) / bd));
+  }
+  kern<<<grid, bd, smem, st>>>(P);
   return cudaGetLastError();
 }
 
