@@ -935,12 +935,12 @@ def main():
     hY = pinned_f(scene.Y, np.float32)
     hGt, hGr, hRo = (pinned_f(a, np.float64) for a in (scene.Gt, scene.Gr, scene.Ro))
     hdelay = pinned_f(np.zeros((1, 1)), np.float64)
-    e2e_steps = max(3, args.steps // 2)
+    e2e_steps = max(10, args.steps)
 
     def e2e_call():
         return das_mixed(hY, hGt, hGr, hRo, scene.dt, hdelay, scene.cp, "tfm", "ignore", "cuda", "f32")
 
-    for _ in range(2):
+    for _ in range(max(3, args.warmup)):
         e2e_call()
     torch.cuda.synchronize()
     if world > 1:

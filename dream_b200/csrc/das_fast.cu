@@ -989,6 +989,10 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
   frexpf(mx, &E);
   const float qscale = ldexpf(1.0f, 22 - E), iS = ldexpf(1.0f, E - 22);
   const int xn = __float2int_rn(xn_f * qscale);
+  // flush: a fixed group of nthr / JC threads per window row (one division
+  // per tile, none per cell)
+  const int tpr = nthr / JC;
+  const int fr = tid / tpr, fq = tid - fr * tpr;
   for (int i0 = T.i_lo; i0 < T.i_hi; i0 += JC) {
     const int jn = min(JC, T.i_hi - i0);
     bool bad = false;
@@ -1007,9 +1011,12 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
         for (int o = 0; o < n_out; o++) exact_scatter<WEIGHTED>(P, T.px, o, i0, jn, n_in, xn_f, Ya);
       continue;
     }
+    // the high word of B64[j] starts at row j of the window: the sum's high
+    // word is the term's window cell
     uint64_t B64[JC];
 #pragma unroll
-    for (int j = 0; j < JC; j++) B64[j] = (j < jn) ? ((uint64_t)S.brel[j * nthr + tid] << F.lo_shift) : 0;
+    for (int j = 0; j < JC; j++)
+      B64[j] = (j < jn) ? ((uint64_t)S.brel[j * nthr + tid] << F.lo_shift) + ((uint64_t)(j * WS) << 32) : 0;
     for (int o = 0; o < n_out; o++) {
       const uint64_t A64 = (uint64_t)S.arel[o * nthr + tid] << F.lo_shift;
       uint64_t sj[JC];
@@ -1033,48 +1040,43 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
         } else {
 #pragma unroll
           for (int j = 0; j < JC; j++)
-            if (j < jn) atomicAdd(win + j * WS + (int)(sj[j] >> 32), xn);
+            if (j < jn) atomicAdd(win + (uint32_t)(sj[j] >> 32), xn);
         }
       }
       __syncthreads();
-      const int64_t colo = ycol_outer(P, n_in, o);
-      if (vec) {
-        const int w4 = WS >> 2;
-        for (int e = tid; e < jn * w4; e += nthr) {
-          const int j = e / w4, t4 = (e - j * w4) << 2;
-          int4 *wp = reinterpret_cast<int4 *>(win + j * WS + t4);
-          const int4 vi = *wp;
-          *wp = make_int4(0, 0, 0, 0);
-          if (vi.x | vi.y | vi.z | vi.w) {
-            float4 v = make_float4((float)vi.x * iS, (float)vi.y * iS, (float)vi.z * iS, (float)vi.w * iS);
-            const int64_t col = colo + ycol_inner(P, i0 + j);
-            const int64_t k0 = (int64_t)S.base[o] + S.base[n_out + i0 + j] + t4;  // a multiple of 4
-            if (WEIGHTED) {
-              const float wc = __ldg(P.w + col);
-              v.x *= wc;
-              v.y *= wc;
-              v.z *= wc;
-              v.w *= wc;
-            }
-            if (k0 >= 0 && k0 + 4 <= K) {
-              red_add_v4(Ya + col * K + k0, v);
-            } else {  // a window edge beyond the A-scan holds only zeros; added one by one to stay inside
-              const float vv[4] = {v.x, v.y, v.z, v.w};
-              for (int q = 0; q < 4; q++)
-                if (vv[q] != 0.0f && k0 + q >= 0 && k0 + q < K) atomicAdd(Ya + col * K + k0 + q, vv[q]);
+      if (fr < jn) {
+        // row fr of the window: sample kb + t of column col
+        const int64_t col = ycol_outer(P, n_in, o) + ycol_inner(P, i0 + fr);
+        const int64_t kb = (int64_t)S.base[o] + S.base[n_out + i0 + fr];  // a multiple of 4
+        const float sc = WEIGHTED ? iS * __ldg(P.w + col) : iS;  // iS a power of two: one rounding either way
+        int *wrow = win + fr * WS;
+        float *ycl = Ya + col * K;
+        if (vec) {
+          for (int t = fq * 4; t < WS; t += tpr * 4) {
+            int4 *wp = reinterpret_cast<int4 *>(wrow + t);
+            const int4 vi = *wp;
+            if (vi.x | vi.y | vi.z | vi.w) {
+              *wp = make_int4(0, 0, 0, 0);
+              const float4 v = make_float4((float)vi.x * sc, (float)vi.y * sc, (float)vi.z * sc, (float)vi.w * sc);
+              const int64_t k0 = kb + t;
+              if (k0 >= 0 && k0 + 4 <= K) {
+                red_add_v4(ycl + k0, v);
+              } else {  // a window edge beyond the A-scan holds only zeros; added one by one to stay inside
+                const float vv[4] = {v.x, v.y, v.z, v.w};
+                for (int q = 0; q < 4; q++)
+                  if (vv[q] != 0.0f && k0 + q >= 0 && k0 + q < K) atomicAdd(ycl + k0 + q, vv[q]);
+              }
             }
           }
-        }
-      } else {
-        for (int e = tid; e < jn * WS; e += nthr) {
-          const int j = e / WS, t = e - j * WS;
-          const float v = (float)win[e] * iS;
-          win[e] = 0;
-          if (v != 0.0f) {
-            const int64_t col = colo + ycol_inner(P, i0 + j);
-            int64_t k = (int64_t)S.base[o] + S.base[n_out + i0 + j] + t;
-            if (k == -1) k = 0;  // p in (-1, 0): sample 0 after truncation toward zero
-            if (k >= 0 && k < K) atomicAdd(Ya + col * K + k, WEIGHTED ? __ldg(P.w + col) * v : v);
+        } else {
+          for (int t = fq; t < WS; t += tpr) {
+            const int vi = wrow[t];
+            if (vi != 0) {
+              wrow[t] = 0;
+              int64_t k = kb + t;
+              if (k == -1) k = 0;  // p in (-1, 0): sample 0 after truncation toward zero
+              if (k >= 0 && k < K) atomicAdd(ycl + k, (float)vi * sc);
+            }
           }
         }
       }
