@@ -617,6 +617,7 @@ __device__ __forceinline__ void tile_setup(const FastParams &P, int64_t tfi, int
   if (!exact_tile) {
     // ---- 2. outer legs, relative to their bases, plus the delta shift ----
     int leg_bad = 0;
+#pragma unroll 4
     for (int o = 0; o < n_out; o++) {
       double dx, dy, dz;
       leg_diffs(P, px, true, o, dx, dy, dz);
@@ -974,6 +975,8 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
   const TileShared &S = T.S;
   const FixFmt F = T.F;
   const int tid = T.tid, nthr = T.nthr, n_out = T.n_out, n_in = T.n_in;
+  const bool active = T.active;
+  const Pixel px = T.px;
   const bool vec = !CHECKED && ((K & 3) == 0) && ((reinterpret_cast<uintptr_t>(Ya) & 15) == 0);
   // fixed-point scale of the tile: max |x| < 2^E, values scaled by 2^(22 - E)
   float mx = fabsf(xn_f);
@@ -1000,15 +1003,15 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
     for (int j = 0; j < jn; j++) {
       const int i = i0 + j;
       double dx, dy, dz;
-      leg_diffs(P, T.px, false, i, dx, dy, dz);
+      leg_diffs(P, px, false, i, dx, dy, dz);
       const uint32_t r = leg_fix(dx, dy, dz, T.cfix, T.dfixB) - ((uint32_t)S.base[n_out + i] << F.fb);
       bad |= r >= ((uint32_t)(S.ext[n_out + i] + 1) << F.fb);
       S.brel[j * nthr + tid] = r;
     }
     if (__syncthreads_or(bad)) {
       // an inner leg outside the tile's bound: this chunk through the exact indices, straight to Ya
-      if (T.active)
-        for (int o = 0; o < n_out; o++) exact_scatter<WEIGHTED>(P, T.px, o, i0, jn, n_in, xn_f, Ya);
+      if (active)
+        for (int o = 0; o < n_out; o++) exact_scatter<WEIGHTED>(P, px, o, i0, jn, n_in, xn_f, Ya);
       continue;
     }
     // the high word of B64[j] starts at row j of the window: the sum's high
@@ -1017,6 +1020,11 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
 #pragma unroll
     for (int j = 0; j < JC; j++)
       B64[j] = (j < jn) ? ((uint64_t)S.brel[j * nthr + tid] << F.lo_shift) + ((uint64_t)(j * WS) << 32) : 0;
+    const bool full = jn == JC;
+    // this thread's flush row fr: the inner element's part of its column, base and extent
+    const bool my_row = fr < jn;
+    const int64_t col_r = my_row ? ycol_inner(P, i0 + fr) : 0;
+    const int base_r = my_row ? S.base[n_out + i0 + fr] : 0, ext_r = my_row ? S.ext[n_out + i0 + fr] : 0;
     for (int o = 0; o < n_out; o++) {
       const uint64_t A64 = (uint64_t)S.arel[o * nthr + tid] << F.lo_shift;
       uint64_t sj[JC];
@@ -1024,35 +1032,41 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
 #pragma unroll
       for (int j = 0; j < JC; j++) {
         sj[j] = A64 + B64[j];
-        if (j < jn) m = min(m, (uint32_t)sj[j]);
+        if (full || j < jn) m = min(m, (uint32_t)sj[j]);
       }
-      if (T.active) {
-        if (m < F.amb_lo) {
-          // an ambiguous term: this outer element's chunk at the exact indices
-          for (int j = 0; j < jn; j++) {
-            int k;
-            if (exact_index(P, T.px, o, i0 + j, k)) {
-              const int slot = k - (S.base[o] + S.base[n_out + i0 + j]);
-              if (slot >= 0 && slot < WS) atomicAdd(win + j * WS + slot, xn);
-              else atomicAdd(Ya + ycol(P, n_in, o, i0 + j) * K + k, WEIGHTED ? __ldg(P.w + ycol(P, n_in, o, i0 + j)) * xn_f : xn_f);
-            }
+      // Inactive lanes carry x = 0 and add nothing, so they need no test.
+      if (m < F.amb_lo) {
+        // an ambiguous term: this outer element's chunk at the exact indices
+        for (int j = 0; j < jn; j++) {
+          int k;
+          if (exact_index(P, px, o, i0 + j, k)) {
+            const int slot = k - (S.base[o] + S.base[n_out + i0 + j]);
+            const int wr = (S.ext[o] + S.ext[n_out + i0 + j] + 4 + 3) & ~3;  // the row's flushed width
+            if (slot >= 0 && slot < wr) atomicAdd(win + j * WS + slot, xn);
+            else atomicAdd(Ya + ycol(P, n_in, o, i0 + j) * K + k, WEIGHTED ? __ldg(P.w + ycol(P, n_in, o, i0 + j)) * xn_f : xn_f);
           }
-        } else {
-#pragma unroll
-          for (int j = 0; j < JC; j++)
-            if (j < jn) atomicAdd(win + (uint32_t)(sj[j] >> 32), xn);
         }
+      } else if (full) {
+        // a full chunk: sixteen (or eight) unguarded additions, no branches
+#pragma unroll
+        for (int j = 0; j < JC; j++) atomicAdd(win + (uint32_t)(sj[j] >> 32), xn);
+      } else {
+#pragma unroll
+        for (int j = 0; j < JC; j++)
+          if (j < jn) atomicAdd(win + (uint32_t)(sj[j] >> 32), xn);
       }
       __syncthreads();
-      if (fr < jn) {
-        // row fr of the window: sample kb + t of column col
-        const int64_t col = ycol_outer(P, n_in, o) + ycol_inner(P, i0 + fr);
-        const int64_t kb = (int64_t)S.base[o] + S.base[n_out + i0 + fr];  // a multiple of 4
+      if (my_row) {
+        // row fr of the window: sample kb + t of column col; the terms of
+        // (o, i) lie in its first ext_o + ext_i + 3 cells
+        const int64_t col = ycol_outer(P, n_in, o) + col_r;
+        const int64_t kb = (int64_t)S.base[o] + base_r;  // a multiple of 4
+        const int wr = (S.ext[o] + ext_r + 4 + 3) & ~3;
         const float sc = WEIGHTED ? iS * __ldg(P.w + col) : iS;  // iS a power of two: one rounding either way
         int *wrow = win + fr * WS;
         float *ycl = Ya + col * K;
         if (vec) {
-          for (int t = fq * 4; t < WS; t += tpr * 4) {
+          for (int t = fq * 4; t < wr; t += tpr * 4) {
             int4 *wp = reinterpret_cast<int4 *>(wrow + t);
             const int4 vi = *wp;
             if (vi.x | vi.y | vi.z | vi.w) {
@@ -1069,7 +1083,7 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
             }
           }
         } else {
-          for (int t = fq; t < WS; t += tpr) {
+          for (int t = fq; t < wr; t += tpr) {
             const int vi = wrow[t];
             if (vi != 0) {
               wrow[t] = 0;
