@@ -236,14 +236,16 @@ def test_rca_full_config(storage, tol):
 @pytest.mark.parametrize("storage", ["f32", "bf16"])
 @pytest.mark.parametrize("spec", [
     dict(kind="tfm", kw=dict(seed=71, n_el=40, K=1800, nx=48, nz=40)),
+    dict(kind="tfm", kw=dict(seed=74, n_el=41, K=1800, nx=40, nz=36)),
     dict(kind="rca", kw=dict(seed=72, n_cols=32, n_rows=32, K=2600, nx=6, ny=6, nz=10, method="rca_rowtx")),
     dict(kind="rca", kw=dict(seed=73, n_cols=32, n_rows=32, K=2600, nx=6, ny=6, nz=10, method="rca_coltx")),
-], ids=["tfm", "rca_rowtx", "rca_coltx"])
+], ids=["tfm", "tfm_odd", "rca_rowtx", "rca_coltx"])
 def test_pipelined_host_upload_matches_device_path(spec, storage):
     """Host arrays (>= 8 MB of A-scans) through the C ABI's host entry
-    (dream_das_run), which uploads them in chunks that overlap the
-    beamforming; the image equals the device-pointer path's up to the order in
-    which the chunks' partial images are added."""
+    (dream_das_run), which uploads them in chunks of inner elements (41
+    elements: uneven chunk widths) that overlap the beamforming; the image
+    equals the device-pointer path's up to the order in which the chunks'
+    partial images are added."""
     import ctypes
     from dream_b200 import _lib
     from dream_b200.beamformer import _fast_plan, das_mixed, grid_hint, parse_method
