@@ -670,7 +670,8 @@ def tfm_extras(dev, scene, plain_f64_ms: float, Im_f64, steps: int = 10, n_copie
 
 
 CASES = ("fast_f32", "fast_bf16", "plain_f64", "plain_f32", "saft_fast", "saft_plain_f64", "uni_f32",
-         "batch", "op_gather", "op_adjoint", "op_wgrad", "op_backward", "adjoint_tfm", "rca_bf16", "rca_f32", "conv_dp",
+         "batch", "op_gather", "op_adjoint", "op_wgrad", "op_backward", "adjoint_tfm", "rca_bf16", "rca_f32",
+         "rca_plain_f32", "conv_dp",
          "conv_pulse", "sir_field", "sir_arr", "conv_fmc")
 
 
@@ -685,6 +686,7 @@ def run_case(name: str, repeat: int = 3):
       op_gather / op_adjoint / op_wgrad / op_backward  CG configuration 32x32, K=2048, 256x256
       adjoint_tfm                                    the operator's adjoint on the TFM 64x64, K=3000, 512x512 frame
       rca_bf16 / rca_f32                             RCA 128x128 row-tx, K=4096, 128x128x256 grid
+      rca_plain_f32                                  the same frame through the plain FP32 kernel (das_f)
       conv_dp / conv_pulse                           fftconv_p of the TFM synthesis: 2000x101 SIRs with a
                                                      2000-sample column / 3999x101 with the 150-sample pulse
       sir_field                                      dreamrect, the reference bench_dreamrect element on a
@@ -748,6 +750,12 @@ def run_case(name: str, repeat: int = 3):
         op = DASOperator(sc.Gt, sc.Gr, sc.Ro, sc.dt, sc.delay, sc.cp, "tfm", sc.Y.shape[0], device=dev)
         x = torch.randn(op.No, device=dev, generator=torch.Generator(device=dev).manual_seed(3))
         fn = lambda: op.adjoint(x)
+    elif name == "rca_plain_f32":
+        Yr, Gc, Grow, Ro = synth.rca_frame_torch(device=dev)
+        f32 = lambda a: torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=np.float32).T)).to(dev).t()
+        Gc32, Gr32, Ro32, d32 = f32(Gc), f32(Grow), f32(Ro), f32(np.zeros((1, 1)))
+        fn = lambda: das_f.das(Yr, Gc32, Gr32, Ro32, np.float32(0.025), d32, np.float32(1480.0), "rca_rowtx",
+                               "ignore", "cuda:0")
     elif name in ("rca_bf16", "rca_f32"):
         Yr, Gc, Grow, Ro = synth.rca_frame_torch(device=dev)
         if name == "rca_bf16":
