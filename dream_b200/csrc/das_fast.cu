@@ -316,8 +316,9 @@ __device__ __noinline__ float exact_partial(const FastParams &P, const Pixel &px
 // issued unconditionally: in an in-bounds tile every floor index, ambiguous
 // or not, lies inside its A-scan. Ambiguity is tracked as the minimum
 // fraction word; a chunk whose minimum falls in the band is recomputed. The
-// minimum runs as four interleaved chains and the packed sums as a tree, so
-// no long dependency chain holds the warp.
+// minimum runs as four interleaved chains, two terms per step (one
+// three-input minimum), and the packed sums as a tree, so no long dependency
+// chain holds the warp; one branch tests all NO outer elements.
 template <class YT, bool WEIGHTED, bool CHECKED, bool FULL, int JC, int NO>
 __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &px, const uint64_t (&B64)[JC],
                                              const uint64_t (&A64)[NO], int o0, int i0, int jn, int n_in,
@@ -340,7 +341,12 @@ __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &p
       y[q][j] = 0.0f;
       if (FULL || j < jn) {
         const uint64_t s = A64[q] + B64[j];
-        mlo[q][j % NM] = min(mlo[q][j % NM], (uint32_t)s);
+        if (FULL && (j & 1)) {  // pairs: one three-input minimum per two terms
+          const uint32_t prev = (uint32_t)(A64[q] + B64[j - 1]);
+          mlo[q][(j >> 1) % NM] = min(mlo[q][(j >> 1) % NM], min(prev, (uint32_t)s));
+        } else if (!FULL) {
+          mlo[q][j % NM] = min(mlo[q][j % NM], (uint32_t)s);
+        }
         const uint32_t off = (uint32_t)(s >> 32);
         if (CHECKED) {
           // Outside the ambiguity band the floor index is exact: [0, K) is in
@@ -399,16 +405,25 @@ __device__ __forceinline__ float chunk_terms(const FastParams &P, const Pixel &p
     }
     partq[q] = part;
   }
+  uint32_t mm = minlo[0];
 #pragma unroll
-  for (int q = 0; q < NO; q++) {
-    if (minlo[q] < amb_lo) {
-      // this outer element's partial is replaced by the exact one (which counts its own OOB)
-      partq[q] = exact_partial<YT, WEIGHTED>(P, px, o0 + q, i0, jn, n_in, oob);
-    } else {
-      oob += oob_chunk[q];
+  for (int q = 1; q < NO; q++) mm = min(mm, minlo[q]);
+  if (mm < amb_lo) {
+#pragma unroll
+    for (int q = 0; q < NO; q++) {
+      if (minlo[q] < amb_lo) {
+        // this outer element's partial is replaced by the exact one (which counts its own OOB)
+        partq[q] = exact_partial<YT, WEIGHTED>(P, px, o0 + q, i0, jn, n_in, oob);
+      } else {
+        oob += oob_chunk[q];
+      }
     }
-    total += partq[q];
+  } else {
+#pragma unroll
+    for (int q = 0; q < NO; q++) oob += oob_chunk[q];
   }
+#pragma unroll
+  for (int q = 0; q < NO; q++) total += partq[q];
   return total;
 }
 
@@ -448,8 +463,17 @@ __device__ __forceinline__ void tile_loop(const FastParams &P, const Pixel &px, 
       continue;
     }
     if (jn == JC) {
-      // compensation every two outer elements
+      // compensation every four outer elements
       int o = 0;
+      for (; o + 4 <= n_out; o += 4) {
+        const uint64_t A2[2] = {((uint64_t)S.arel[o * nthr + tid] << F.lo_shift) + ((uint64_t)S.ahi[o] << 32),
+                                ((uint64_t)S.arel[(o + 1) * nthr + tid] << F.lo_shift) + ((uint64_t)S.ahi[o + 1] << 32)};
+        const float p0 = chunk_terms<YT, WEIGHTED, CHECKED, true, JC, 2>(P, px, B64, A2, o, i0, JC, n_in, F.amb_lo, oob);
+        const uint64_t A3[2] = {((uint64_t)S.arel[(o + 2) * nthr + tid] << F.lo_shift) + ((uint64_t)S.ahi[o + 2] << 32),
+                                ((uint64_t)S.arel[(o + 3) * nthr + tid] << F.lo_shift) + ((uint64_t)S.ahi[o + 3] << 32)};
+        const float p1 = chunk_terms<YT, WEIGHTED, CHECKED, true, JC, 2>(P, px, B64, A3, o + 2, i0, JC, n_in, F.amb_lo, oob);
+        neumaier(acc_s, acc_c, p0 + p1);
+      }
       for (; o + 2 <= n_out; o += 2) {
         const uint64_t A2[2] = {((uint64_t)S.arel[o * nthr + tid] << F.lo_shift) + ((uint64_t)S.ahi[o] << 32),
                                 ((uint64_t)S.arel[(o + 1) * nthr + tid] << F.lo_shift) + ((uint64_t)S.ahi[o + 1] << 32)};
