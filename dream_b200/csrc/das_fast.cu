@@ -970,9 +970,10 @@ __device__ __forceinline__ void scatter_loop(const FastParams &P, const TileCtx 
 }
 
 
-// Columns per shared-memory window batch and samples per window (windows
-// wider than this send their tile to the direct-reduction path).
-constexpr int SCATTER_WCAP = 256;
+// Samples per shared-memory window row (windows wider than this send their
+// tile to the direct-reduction path). Two buffers of JC rows alternate, so
+// 256-point tiles of 64 outer elements keep two CTAs per SM.
+constexpr int SCATTER_WCAP = 192;
 
 __device__ __forceinline__ void red_add_v4(float *p, float4 v) {
   asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
@@ -1007,7 +1008,7 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
   for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
   __shared__ float s_mx[8];
   if ((tid & 31) == 0) s_mx[tid >> 5] = mx;
-  for (int e = tid; e < JC * WS; e += nthr) win[e] = 0;
+  for (int e = tid; e < 2 * JC * WS; e += nthr) win[e] = 0;
   __syncthreads();
   mx = 0.0f;
   for (int w = 0; w < (nthr >> 5); w++) mx = fmaxf(mx, s_mx[w]);
@@ -1020,6 +1021,11 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
   // per tile, none per cell)
   const int tpr = nthr / JC;
   const int fr = tid / tpr, fq = tid - fr * tpr;
+  // Two window buffers alternate per (outer element, chunk): the adds of one
+  // batch and the flush of the previous one need only the barrier between a
+  // batch's adds and its flush (a buffer is added to again only after the
+  // next batch's barrier, which every thread reaches after its flush).
+  int it = 0;
   for (int i0 = T.i_lo; i0 < T.i_hi; i0 += JC) {
     const int jn = min(JC, T.i_hi - i0);
     bool bad = false;
@@ -1051,6 +1057,7 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
     const int base_r = my_row ? S.base[n_out + i0 + fr] : 0, ext_r = my_row ? S.ext[n_out + i0 + fr] : 0;
     for (int o = 0; o < n_out; o++) {
       const uint64_t A64 = (uint64_t)S.arel[o * nthr + tid] << F.lo_shift;
+      int *wb = win + (it & 1) * (JC * WS);  // this batch's buffer
       uint64_t sj[JC];
       uint32_t m = 0xffffffffu;
 #pragma unroll
@@ -1066,18 +1073,18 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
           if (exact_index(P, px, o, i0 + j, k)) {
             const int slot = k - (S.base[o] + S.base[n_out + i0 + j]);
             const int wr = (S.ext[o] + S.ext[n_out + i0 + j] + 4 + 3) & ~3;  // the row's flushed width
-            if (slot >= 0 && slot < wr) atomicAdd(win + j * WS + slot, xn);
+            if (slot >= 0 && slot < wr) atomicAdd(wb + j * WS + slot, xn);
             else atomicAdd(Ya + ycol(P, n_in, o, i0 + j) * K + k, WEIGHTED ? __ldg(P.w + ycol(P, n_in, o, i0 + j)) * xn_f : xn_f);
           }
         }
       } else if (full) {
         // a full chunk: sixteen (or eight) unguarded additions, no branches
 #pragma unroll
-        for (int j = 0; j < JC; j++) atomicAdd(win + (uint32_t)(sj[j] >> 32), xn);
+        for (int j = 0; j < JC; j++) atomicAdd(wb + (uint32_t)(sj[j] >> 32), xn);
       } else {
 #pragma unroll
         for (int j = 0; j < JC; j++)
-          if (j < jn) atomicAdd(win + (uint32_t)(sj[j] >> 32), xn);
+          if (j < jn) atomicAdd(wb + (uint32_t)(sj[j] >> 32), xn);
       }
       __syncthreads();
       if (my_row) {
@@ -1087,7 +1094,7 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
         const int64_t kb = (int64_t)S.base[o] + base_r;  // a multiple of 4
         const int wr = (S.ext[o] + ext_r + 4 + 3) & ~3;
         const float sc = WEIGHTED ? iS * __ldg(P.w + col) : iS;  // iS a power of two: one rounding either way
-        int *wrow = win + fr * WS;
+        int *wrow = wb + fr * WS;
         float *ycl = Ya + col * K;
         if (vec) {
           for (int t = fq * 4; t < wr; t += tpr * 4) {
@@ -1118,7 +1125,7 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
           }
         }
       }
-      __syncthreads();
+      it++;
     }
   }
 }
@@ -1154,7 +1161,7 @@ __global__ void __launch_bounds__(256, 2) das_scatter_kernel(const FastParams P,
 cudaError_t launch_scatter(const FastParams &P, const float *X, float *Ya, cudaStream_t st) {
   const int nthr = P.tile_f * P.tile_s;
   // the tile's arrays, then the windows of one (outer, inner chunk) batch
-  const size_t smem = fast_smem_bytes(P, nthr) + (size_t)(P.jc == 8 ? 8 : 16) * SCATTER_WCAP * sizeof(float);
+  const size_t smem = fast_smem_bytes(P, nthr) + 2 * (size_t)(P.jc == 8 ? 8 : 16) * SCATTER_WCAP * sizeof(float);
   auto kern = P.w ? (P.jc == 8 ? das_scatter_kernel<true, 8> : das_scatter_kernel<true, 16>)
                   : (P.jc == 8 ? das_scatter_kernel<false, 8> : das_scatter_kernel<false, 16>);
   cudaError_t e = ensure_smem(kern, smem);
