@@ -694,6 +694,7 @@ __device__ __forceinline__ void fast_tile(const FastParams &P, int64_t tfi, int6
   float acc_s = 0.0f, acc_c = 0.0f;
   unsigned int oob = 0;
   const YT *__restrict__ Yp = reinterpret_cast<const YT *>(P.Y);
+  const Pixel px = T.px;  // a copy for the calls that take it by reference
   if (T.exact_tile) {
     // every term through the exact FP64 index
     for (int o = 0; o < T.n_out; o++) {
@@ -701,7 +702,7 @@ __device__ __forceinline__ void fast_tile(const FastParams &P, int64_t tfi, int6
       for (int i = T.i_lo; i < T.i_hi; i++) {
         int k;
         const int64_t col = ycol(P, T.n_in, o, i);
-        if (exact_index(P, T.px, o, i, k)) {
+        if (exact_index(P, px, o, i, k)) {
           float y = load_sample(Yp + col * P.K + k);
           part = WEIGHTED ? fmaf(__ldg(P.w + col), y, part) : part + y;
         } else {
@@ -711,10 +712,10 @@ __device__ __forceinline__ void fast_tile(const FastParams &P, int64_t tfi, int6
       neumaier(acc_s, acc_c, part);
     }
   } else if (T.in_bounds) {
-    tile_loop<YT, WEIGHTED, false, JC>(P, T.px, T.S, T.F, T.cfix, T.dfixB, T.tid, T.nthr, T.n_out, T.n_in, T.i_lo,
+    tile_loop<YT, WEIGHTED, false, JC>(P, px, T.S, T.F, T.cfix, T.dfixB, T.tid, T.nthr, T.n_out, T.n_in, T.i_lo,
                                        T.i_hi, acc_s, acc_c, oob);
   } else {
-    tile_loop<YT, WEIGHTED, true, JC>(P, T.px, T.S, T.F, T.cfix, T.dfixB, T.tid, T.nthr, T.n_out, T.n_in, T.i_lo,
+    tile_loop<YT, WEIGHTED, true, JC>(P, px, T.S, T.F, T.cfix, T.dfixB, T.tid, T.nthr, T.n_out, T.n_in, T.i_lo,
                                       T.i_hi, acc_s, acc_c, oob);
   }
   if (T.active) P.Im[T.no] = P.accumulate ? P.Im[T.no] + (acc_s + acc_c) : acc_s + acc_c;
@@ -910,6 +911,7 @@ __device__ __forceinline__ void scatter_loop(const FastParams &P, const TileCtx 
   const TileShared &S = T.S;
   const FixFmt F = T.F;
   const int tid = T.tid, nthr = T.nthr, n_out = T.n_out, n_in = T.n_in;
+  const Pixel px = T.px;  // a copy for the exact path (by reference), so T stays in registers
   for (int i0 = T.i_lo; i0 < T.i_hi; i0 += JC) {
     const int jn = min(JC, T.i_hi - i0);
     bool bad = false;
@@ -917,14 +919,14 @@ __device__ __forceinline__ void scatter_loop(const FastParams &P, const TileCtx 
     for (int j = 0; j < jn; j++) {
       const int i = i0 + j;
       double dx, dy, dz;
-      leg_diffs(P, T.px, false, i, dx, dy, dz);
+      leg_diffs(P, px, false, i, dx, dy, dz);
       const uint32_t r = leg_fix(dx, dy, dz, T.cfix, T.dfixB) - ((uint32_t)S.base[n_out + i] << F.fb);
       bad |= r >= ((uint32_t)(S.ext[n_out + i] + 1) << F.fb);
       S.brel[j * nthr + tid] = r;
     }
     if (__any_sync(0xffffffffu, bad)) {
       if (T.active)
-        for (int o = 0; o < n_out; o++) exact_scatter<WEIGHTED>(P, T.px, o, i0, jn, n_in, xn, Ya);
+        for (int o = 0; o < n_out; o++) exact_scatter<WEIGHTED>(P, px, o, i0, jn, n_in, xn, Ya);
       continue;
     }
     uint64_t B64[JC];
@@ -946,7 +948,7 @@ __device__ __forceinline__ void scatter_loop(const FastParams &P, const TileCtx 
         if (j < jn) m = min(m, (uint32_t)sj[j]);
       }
       if (m < F.amb_lo) {  // an ambiguous term: this outer element's chunk through the exact indices
-        if (T.active) exact_scatter<WEIGHTED>(P, T.px, o, i0, jn, n_in, xn, Ya);
+        if (T.active) exact_scatter<WEIGHTED>(P, px, o, i0, jn, n_in, xn, Ya);
         continue;
       }
       const int64_t colo = ycol_outer(P, n_in, o);
@@ -1143,10 +1145,11 @@ __global__ void __launch_bounds__(256, 2) das_scatter_kernel(const FastParams P,
     if (T.in_bounds) scatter_window_loop<WEIGHTED, false, JC>(P, T, xn, Ya, win, WS);
     else scatter_window_loop<WEIGHTED, true, JC>(P, T, xn, Ya, win, WS);
   } else if (T.exact_tile) {
+    const Pixel px = T.px;  // a copy: the exact path takes it by reference, T stays in registers
     if (T.active)
       for (int o = 0; o < T.n_out; o++)
         for (int i0 = T.i_lo; i0 < T.i_hi; i0 += 16)
-          exact_scatter<WEIGHTED>(P, T.px, o, i0, min(16, T.i_hi - i0), T.n_in, xn, Ya);
+          exact_scatter<WEIGHTED>(P, px, o, i0, min(16, T.i_hi - i0), T.n_in, xn, Ya);
   } else if (T.in_bounds) {
     scatter_loop<WEIGHTED, false, JC>(P, T, xn, Ya);
   } else {
