@@ -1061,12 +1061,18 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
       const uint64_t A64 = (uint64_t)S.arel[o * nthr + tid] << F.lo_shift;
       int *wb = win + (it & 1) * (JC * WS);  // this batch's buffer
       uint64_t sj[JC];
-      uint32_t m = 0xffffffffu;
+      uint32_t mc[2] = {0xffffffffu, 0xffffffffu};  // two chains, two terms per step
 #pragma unroll
-      for (int j = 0; j < JC; j++) {
-        sj[j] = A64 + B64[j];
-        if (full || j < jn) m = min(m, (uint32_t)sj[j]);
+      for (int j = 0; j < JC; j++) sj[j] = A64 + B64[j];
+      if (full) {
+#pragma unroll
+        for (int j = 0; j < JC; j += 2) mc[(j >> 1) & 1] = min(mc[(j >> 1) & 1], min((uint32_t)sj[j], (uint32_t)sj[j + 1]));
+      } else {
+#pragma unroll
+        for (int j = 0; j < JC; j++)
+          if (j < jn) mc[0] = min(mc[0], (uint32_t)sj[j]);
       }
+      const uint32_t m = min(mc[0], mc[1]);
       // Inactive lanes carry x = 0 and add nothing, so they need no test.
       if (m < F.amb_lo) {
         // an ambiguous term: this outer element's chunk at the exact indices
