@@ -1060,22 +1060,31 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
     for (int o = 0; o < n_out; o++) {
       const uint64_t A64 = (uint64_t)S.arel[o * nthr + tid] << F.lo_shift;
       int *wb = win + (it & 1) * (JC * WS);  // this batch's buffer
-      uint64_t sj[JC];
+      // Adds first, ambiguity test after: in the rare ambiguous batch the same
+      // integer values are taken back out of the same cells (exact) and the
+      // chunk goes through the exact indices, so no term's sum is kept.
       uint32_t mc[2] = {0xffffffffu, 0xffffffffu};  // two chains, two terms per step
-#pragma unroll
-      for (int j = 0; j < JC; j++) sj[j] = A64 + B64[j];
       if (full) {
 #pragma unroll
-        for (int j = 0; j < JC; j += 2) mc[(j >> 1) & 1] = min(mc[(j >> 1) & 1], min((uint32_t)sj[j], (uint32_t)sj[j + 1]));
+        for (int j = 0; j < JC; j += 2) {
+          const uint64_t s0 = A64 + B64[j], s1 = A64 + B64[j + 1];
+          atomicAdd(wb + (uint32_t)(s0 >> 32), xn);
+          atomicAdd(wb + (uint32_t)(s1 >> 32), xn);
+          mc[(j >> 1) & 1] = min(mc[(j >> 1) & 1], min((uint32_t)s0, (uint32_t)s1));
+        }
       } else {
 #pragma unroll
         for (int j = 0; j < JC; j++)
-          if (j < jn) mc[0] = min(mc[0], (uint32_t)sj[j]);
+          if (j < jn) {
+            const uint64_t s0 = A64 + B64[j];
+            atomicAdd(wb + (uint32_t)(s0 >> 32), xn);
+            mc[0] = min(mc[0], (uint32_t)s0);
+          }
       }
-      const uint32_t m = min(mc[0], mc[1]);
       // Inactive lanes carry x = 0 and add nothing, so they need no test.
-      if (m < F.amb_lo) {
-        // an ambiguous term: this outer element's chunk at the exact indices
+      if (min(mc[0], mc[1]) < F.amb_lo) {
+        // an ambiguous term: take this outer element's adds back and use the exact indices
+        for (int j = 0; j < jn; j++) atomicSub(wb + (uint32_t)((A64 + B64[j]) >> 32), xn);
         for (int j = 0; j < jn; j++) {
           int k;
           if (exact_index(P, px, o, i0 + j, k)) {
@@ -1085,14 +1094,6 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
             else atomicAdd(Ya + ycol(P, n_in, o, i0 + j) * K + k, WEIGHTED ? __ldg(P.w + ycol(P, n_in, o, i0 + j)) * xn_f : xn_f);
           }
         }
-      } else if (full) {
-        // a full chunk: sixteen (or eight) unguarded additions, no branches
-#pragma unroll
-        for (int j = 0; j < JC; j++) atomicAdd(wb + (uint32_t)(sj[j] >> 32), xn);
-      } else {
-#pragma unroll
-        for (int j = 0; j < JC; j++)
-          if (j < jn) atomicAdd(wb + (uint32_t)(sj[j] >> 32), xn);
       }
       __syncthreads();
       if (my_row) {

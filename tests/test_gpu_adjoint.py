@@ -65,6 +65,39 @@ def test_operators_match_oracle(method):
     assert torch.allclose(dw2, op.wgrad(xt, Yt), rtol=1e-5, atol=1e-5 * float(np.abs(refw).max()))
 
 
+def test_adjoint_lattice_exact_integer_times():
+    """A lattice of 3-4-5 triangles (cp = 1000 m/s, dt = 1 us) puts many
+    terms' sample positions on, or within rounding of, integers. In the
+    adjoint those terms take the ambiguous-band path: the window additions of
+    their (outer element, chunk) batch are taken back out and the exact FP64
+    indices used instead, so every term must still land where the oracle's
+    index puts it (adjoint and weight gradient)."""
+    from dream_b200.autograd import DASOperator
+    G = np.asfortranarray(np.array([[0.0, 0.0, 0.0], [3.0, 0.0, 0.0], [-4.0, 0.0, 0.0], [6.0, 0.0, 0.0]]))
+    xs = np.arange(-12.0, 12.5, 1.0)
+    zs = np.arange(0.0, 16.5, 1.0)
+    X, Z = np.meshgrid(xs, zs)
+    Ro = np.asfortranarray(np.stack([X.flatten("F"), np.zeros(X.size), Z.flatten("F")], 1))
+    K, dl = 64, np.zeros((1, 1))
+    rng = np.random.default_rng(7)
+    Y = f32(rng.normal(size=(K, 16)))
+    _, _, _, idx = oracle.das(np.asfortranarray(Y), G, G, Ro, 1.0, dl, 1000.0, "tfm", "ignore", np.float64,
+                              return_idx=True)
+    op = DASOperator(G, G.copy(order="F"), Ro, 1.0, dl, 1000.0, "tfm", K)
+    C, No = idx.shape
+    w = f32(rng.uniform(0.3, 1.2, C))
+    x = f32(rng.normal(size=No))
+    Yt = torch.from_numpy(np.ascontiguousarray(Y.T)).float().cuda().t()
+    wt = torch.from_numpy(w).float().cuda()
+    xt = torch.from_numpy(x).float().cuda()
+    Ya = op.adjoint(xt, wt).cpu().double().numpy()
+    refa = oracle.adjoint(idx, x, w, K)
+    assert np.abs(Ya - refa).max() <= 1e-5 * np.abs(refa).max()
+    dw = op.wgrad(xt, Yt).cpu().double().numpy()
+    refw = oracle.wgrad(idx, x, Y)
+    assert np.abs(dw - refw).max() <= 1e-5 * np.abs(refw).max()
+
+
 def test_dot_product_full_cg_config():
     """<DAS_w Y, x> = <Y, DAS_w^T x> on the 32x32, K=2048, 256x256 configuration."""
     from dream_b200 import synth
