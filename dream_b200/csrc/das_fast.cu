@@ -499,6 +499,7 @@ struct TileCtx {
   Pixel px;
   int64_t no;
   bool active, exact_tile, in_bounds;
+  bool vec_safe;  // in bounds, and every scatter window row ends inside its A-scan
   int tid, nthr, n_out, n_in, i_lo, i_hi;
   FixFmt F;
   double cfix, dfixB;
@@ -657,6 +658,8 @@ __device__ __forceinline__ void tile_setup(const FastParams &P, int64_t tfi, int
   T.active = active;
   T.exact_tile = exact_tile;
   T.in_bounds = in_bounds;
+  // a window row ends by base_o + ext_o + base_i + ext_i + 7 <= hiA + hiB + 7
+  T.vec_safe = in_bounds && (int64_t)hiA + hiB + 7 <= P.K;
   T.tid = tid;
   T.nthr = nthr;
   T.n_out = n_out;
@@ -1056,6 +1059,8 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
     // this thread's flush row fr: the inner element's part of its column, base and extent
     const bool my_row = fr < jn;
     const int64_t col_r = my_row ? ycol_inner(P, i0 + fr) : 0;
+    const int64_t ostride = P.ycol_o > 0 ? P.ycol_o : n_in;  // columns per outer element
+    float *ycl = Ya + col_r * K;  // this row's column for outer element o, stepped per o
     const int base_r = my_row ? S.base[n_out + i0 + fr] : 0, ext_r = my_row ? S.ext[n_out + i0 + fr] : 0;
     for (int o = 0; o < n_out; o++) {
       const uint64_t A64 = (uint64_t)S.arel[o * nthr + tid] << F.lo_shift;
@@ -1099,13 +1104,20 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
       if (my_row) {
         // row fr of the window: sample kb + t of column col; the terms of
         // (o, i) lie in its first ext_o + ext_i + 3 cells
-        const int64_t col = ycol_outer(P, n_in, o) + col_r;
         const int64_t kb = (int64_t)S.base[o] + base_r;  // a multiple of 4
         const int wr = (S.ext[o] + ext_r + 4 + 3) & ~3;
-        const float sc = WEIGHTED ? iS * __ldg(P.w + col) : iS;  // iS a power of two: one rounding either way
+        const float sc = WEIGHTED ? iS * __ldg(P.w + o * ostride + col_r) : iS;  // iS a power of two: one rounding either way
         int *wrow = wb + fr * WS;
-        float *ycl = Ya + col * K;
-        if (vec) {
+        if (vec && T.vec_safe) {  // every vector of the row lies inside the A-scan
+          for (int t = fq * 4; t < wr; t += tpr * 4) {
+            int4 *wp = reinterpret_cast<int4 *>(wrow + t);
+            const int4 vi = *wp;
+            if (vi.x | vi.y | vi.z | vi.w) {
+              *wp = make_int4(0, 0, 0, 0);
+              red_add_v4(ycl + kb + t, make_float4((float)vi.x * sc, (float)vi.y * sc, (float)vi.z * sc, (float)vi.w * sc));
+            }
+          }
+        } else if (vec) {
           for (int t = fq * 4; t < wr; t += tpr * 4) {
             int4 *wp = reinterpret_cast<int4 *>(wrow + t);
             const int4 vi = *wp;
@@ -1134,6 +1146,7 @@ __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const T
           }
         }
       }
+      ycl += ostride * K;
       it++;
     }
   }
