@@ -218,7 +218,11 @@ int dream_das_set_grid_hint(dream_das_plan *plan, int64_t n_fast);
  * tile_f points along the fast grid axis x tile_s along the slow axis
  * (tile_f*tile_s threads, 32..256, a multiple of 32; with a grid hint tile_f
  * is a multiple of 8 and tile_s of 4, without one tile_s must be 1).
- * (0, 0) restores the automatic choice. Used by the autotuner.
+ * (0, 0) restores the automatic choice. Used by the autotuner. Automatic,
+ * on a hinted grid: 16 x 8 points for the gathers (8 x 32 for frames of fewer
+ * points than two waves of 128-point tiles, 8 x 128 per SM), 8 x 32 for the
+ * operator's adjoint; 256 consecutive points without a hint; fewer points
+ * when many outer elements would overflow the tile's shared memory.
  */
 int dream_das_set_tile(dream_das_plan *plan, int tile_f, int tile_s);
 int dream_das_get_tile(const dream_das_plan *plan, int *tile_f, int *tile_s);
