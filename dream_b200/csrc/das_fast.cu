@@ -989,14 +989,16 @@ __device__ __forceinline__ void red_add_v4(float *p, float4 v) {
 // elements, every term goes into the shared-memory window of its column (the
 // tile's sample range [base_o + base_i, ... + WS), 16-byte aligned because the
 // bases are multiples of 4); then the windows are added to Ya with 4-wide
-// vector reductions (the weight applied once per sample) and cleared. Two
-// block barriers per (o, chunk). A term's slot is the high word of A64 + B64
-// when both hold only the relative legs. The windows hold fixed-point
+// vector reductions (the weight applied once per sample) and cleared; two
+// buffers alternate, one block barrier per (o, chunk). A term's slot is the
+// high word of A64 + B64 when both hold only the relative legs (the inner leg
+// carrying its row). The windows hold fixed-point
 // integers, x scaled by 2^(22 - E) with max |x| over the tile below 2^E, so
 // the shared-memory additions are native integer atomics, exact and
 // independent of their order (a slot receives at most one term per thread
-// per batch, at most 256 terms of magnitude up to 2^22); each value is
-// rounded once, to within 2^-22 of the tile's largest |x|.
+// per batch, at most 256 terms of magnitude up to 2^22, and a batch taken
+// back subtracts exactly what it added); each value is rounded once, to within
+// 2^-22 of the tile's largest |x|.
 template <bool WEIGHTED, bool CHECKED, int JC>
 __device__ __forceinline__ void scatter_window_loop(const FastParams &P, const TileCtx &T, float xn_f, float *Ya,
                                                     float *winf, int WS) {
@@ -1183,7 +1185,7 @@ __global__ void __launch_bounds__(256, 2) das_scatter_kernel(const FastParams P,
 // for the forward; P.w optional). Ya is not zeroed here.
 cudaError_t launch_scatter(const FastParams &P, const float *X, float *Ya, cudaStream_t st) {
   const int nthr = P.tile_f * P.tile_s;
-  // the tile's arrays, then the windows of one (outer, inner chunk) batch
+  // the tile's arrays, then two buffers of one (outer, inner chunk) batch's windows
   const size_t smem = fast_smem_bytes(P, nthr) + 2 * (size_t)(P.jc == 8 ? 8 : 16) * SCATTER_WCAP * sizeof(float);
   auto kern = P.w ? (P.jc == 8 ? das_scatter_kernel<true, 8> : das_scatter_kernel<true, 16>)
                   : (P.jc == 8 ? das_scatter_kernel<false, 8> : das_scatter_kernel<false, 16>);
