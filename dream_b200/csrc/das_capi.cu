@@ -779,12 +779,14 @@ static int op_scatter(dream_das_plan *p, const float *X, const float *dW, float 
   F.w = dW;
   int r = tile_params(p, F, 0);
   if (r) return r;
-  // The scatter's own automatic tile on a hinted grid: 8 x 32 points, long
-  // along the slow axis, where a column's sample window grows slowest
+  // The scatter's own automatic tile on a hinted TFM grid: 8 x 32 points,
+  // long along the slow axis, where a column's sample window grows slowest
   // relative to the tile's terms (64x64-element TFM frame 1.25 -> 1.20 ms,
-  // 32x32-element CG configuration 0.130 -> 0.120 ms, against 16 x 8).
+  // 32x32-element CG configuration 0.130 -> 0.120 ms, against 16 x 8). RCA
+  // volumes keep the forward's tile: 32 points along their slow axis spread a
+  // stripe's leg beyond the window (128x128 frame: 108.7 against 81.7 ms).
   const int n_out = (F.method == DREAM_DAS_RCA_ROWTX) ? F.Nr : F.Nt;
-  if (p->tile_f == 0 && p->n_fast > 0 && (size_t)n_out * 256 * 4 <= 96 * 1024) {
+  if (p->tile_f == 0 && p->n_fast > 0 && F.method == DREAM_DAS_TFM && (size_t)n_out * 256 * 4 <= 96 * 1024) {
     F.tile_f = 8;
     F.tile_s = 32;
     F.wf = 8;

@@ -221,7 +221,7 @@ int dream_das_set_grid_hint(dream_das_plan *plan, int64_t n_fast);
  * (0, 0) restores the automatic choice. Used by the autotuner. Automatic,
  * on a hinted grid: 16 x 8 points for the gathers (8 x 32 for frames of fewer
  * points than two waves of 128-point tiles, 8 x 128 per SM), 8 x 32 for the
- * operator's adjoint; 256 consecutive points without a hint; fewer points
+ * operator's adjoint on TFM frames; 256 consecutive points without a hint; fewer points
  * when many outer elements would overflow the tile's shared memory.
  */
 int dream_das_set_tile(dream_das_plan *plan, int tile_f, int tile_s);
